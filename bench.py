@@ -1,0 +1,469 @@
+"""Benchmark: batched window queries against a 10M-box tree on one B200 (or N
+replicas), plus the 100M-box bulk load.
+
+Headline (one JSON line on rank 0):
+  metric  window queries/s of the persistent, graph-captured query form
+          (10M uniform boxes, side U[0,1e-3]; 1M windows, side log-uniform in
+          [1e-5, 1e-1], half centred on boxes, half uniform), every hit pair
+          written to HBM.  A step = one pass over the 1M-window batch.
+  plain   the same batch through the plain per-batch form (count pass, scan,
+          write pass; one warp per window in input order).
+  build   100M clustered boxes (1000 Gaussian clusters + 10% uniform,
+          log-normal sides, 1% duplicates, 1% points): encode + radix sort +
+          node build, boxes/s.
+  e2e     the same query metric through the C ABI with host buffers: each step
+          copies the windows from pinned host memory, queries, and copies every
+          hit pair back to pinned host memory.
+  roofline  of the dominant kernel (the persistent traversal): algorithmic bytes
+          16 B per window + 16 B per leaf box tested + 12 B per hit, over its
+          CUDA-event time, against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own CPU brute force (nested_loop_query,
+          compiled from its sources) on the host cores over a bounded sample.
+
+`--impl reference` times that CPU path alone (rank 0) on the same metric.
+All inputs are synthetic and seeded (no dataset is involved).  The box SoA
+(200 MB), the windows and the output (tens of GB) are larger than L2, so no
+flush is needed between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+QUERY_BOXES = 10_000_000
+QUERY_WINDOWS = 1_000_000
+BUILD_BOXES = 100_000_000
+FANOUT = 16
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--boxes", type=int, default=QUERY_BOXES)
+    p.add_argument("--windows", type=int, default=QUERY_WINDOWS)
+    p.add_argument("--build-boxes", type=int, default=BUILD_BOXES)
+    p.add_argument("--fanout", type=int, default=FANOUT)
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        loaded = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path (bounded sample)
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7):
+    """Windows/s of the reference's nested_loop_query over all host threads,
+    on a sample of windows sized to about `seconds` of CPU work.  Falls back to
+    the oracle's restatement when the reference build is absent."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    kind = "reference" if O.ref_cpu_available() else "port"
+    rng = np.random.default_rng(rng_seed)
+
+    def run(m):
+        idx = np.sort(rng.choice(windows.n, size=min(m, windows.n), replace=False))
+        q = windows.take(idx)
+        qid = np.arange(q.n, dtype=np.int32)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            R = O.ref_cpu()
+            a = [np.ascontiguousarray(x) for x in (q.xmin, q.ymin, q.xmax, q.ymax)]
+            d = [np.ascontiguousarray(x) for x in (boxes.xmin, boxes.ymin, boxes.xmax, boxes.ymax)]
+            pairs = R.ref_nested_loop_query_mt(*a, qid, q.n, *d, boxes.id, boxes.n, threads)
+        else:
+            c, _ = O.nested_loop_stats(q, boxes, nthreads=threads)
+            pairs = int(c.sum())
+        return q.n, time.perf_counter() - t0, int(pairs)
+
+    n0, t0, _ = run(threads)
+    m = int(max(threads, min(windows.n, n0 / max(t0, 1e-6) * seconds)))
+    m = (m + threads - 1) // threads * threads
+    n, t, pairs = run(m)
+    return {"value": n / t, "unit": "windows/s", "cores": threads, "kind": kind,
+            "sample": f"{n} of {windows.n} windows x {boxes.n} boxes, {t:.1f} s, {pairs} pairs"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def make_query_inputs(rank: int, nbox: int, nwin: int):
+    from curtree_b200 import datasets as D
+    boxes = D.uniform_boxes(nbox, seed=3)
+    windows = D.mixed_windows(nwin, boxes, seed=103 + 1000 * rank)
+    return boxes, windows
+
+
+def timed(fn, steps, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def profile_collect(name):
+    import ctypes
+    from curtree_b200 import _lib
+    ms = ctypes.c_double(0)
+    n = ctypes.c_int64(0)
+    _lib.load().crt_profile_collect(name.encode() if name else None, ctypes.byref(ms), ctypes.byref(n))
+    return ms.value, n.value
+
+
+def run_ours(args, rank, world, dist):
+    import ctypes
+
+    import torch
+
+    import curtree_b200 as C
+    from curtree_b200 import _lib
+
+    L = _lib.load()
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    skip = set(s for s in args.skip.split(",") if s)
+    hbm_peak, peak_kind = peaks()
+    out = {}
+
+    # ---- inputs resident in HBM -------------------------------------------
+    boxes, windows = make_query_inputs(rank, args.boxes, args.windows)
+    d_in = C.BBox.from_host(boxes)
+    sorted_box, rt = C.build_into(d_in, args.fanout)
+    del d_in
+    d_win = C.BBox.from_host(windows)
+    st = C.query_stats(rt, sorted_box, d_win)
+    pairs, tested = st["hits"], st["tested"]
+    cap = C.query_capacity(pairs)
+    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    res = C.new_result_block()
+
+    # ---- persistent form (graph plan) -------------------------------------
+    L.crt_profile_enable(1)
+    plan = C.Plan(rt, sorted_box, d_win, fid, tid, res)
+    for _ in range(args.warmup):
+        plan.launch()
+    torch.cuda.synchronize()
+    r = C.read_result(res)
+    assert r["overflow"] == 0 and r["count"] == pairs and r["error"] == 0, r
+    profile_collect(None)
+    launches0 = C.kernel_launches()
+    if dist is not None:
+        dist.barrier()
+    with Clocks(dev) as clk:
+        ms = timed(plan.launch, args.steps, stream)
+    launches = C.kernel_launches() - launches0
+    k_ms, k_n = profile_collect("traverse_persistent")
+    profile_collect(None)
+    r = C.read_result(res)
+    assert r["overflow"] == 0 and r["count"] == pairs, r
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    step_ms = ms_max / args.steps
+    kern_ms = k_ms / max(k_n, 1)
+    alg_bytes = 16 * args.windows + 16 * tested + 12 * pairs
+    out["persistent"] = {"ms_per_step": step_ms, "windows_per_s": world * args.windows / (step_ms / 1e3),
+                         "kernel_ms": kern_ms}
+    out["roofline"] = {"bound": "hbm", "achieved": alg_bytes / (kern_ms / 1e3) / 1e9,
+                       "peak": hbm_peak, "unit": "GB/s",
+                       "frac": alg_bytes / (kern_ms / 1e3) / 1e9 / hbm_peak,
+                       "traffic": None, "peak_kind": peak_kind,
+                       "kernel": "persistent_kernel",
+                       "algorithmic_bytes": alg_bytes,
+                       "bytes_model": "16 B/window + 16 B/leaf box tested + 12 B/hit",
+                       "strict_io_bytes": 16 * args.windows + 8 * pairs + 20 * args.boxes}
+    out["clocks"] = clk.summary()
+    out["gpu_launches"] = launches
+    out["workload_stats"] = {"pairs": pairs, "leaf_boxes_tested": tested,
+                             "pairs_per_window": pairs / args.windows}
+    plan.destroy()
+
+    # ---- plain form ---------------------------------------------------------
+    if "plain" not in skip:
+        offs = torch.empty(args.windows + 1, dtype=torch.int64, device="cuda")
+        plain = lambda: C.query_into(rt, sorted_box, d_win, fid, tid, res, offs, C.CRT_QUERY_PLAIN)
+        for _ in range(max(1, args.warmup)):
+            plain()
+        torch.cuda.synchronize()
+        r = C.read_result(res)
+        assert r["overflow"] == 0 and r["count"] == pairs, r
+        profile_collect(None)
+        pms = timed(plain, args.steps, stream)
+        pk_ms, pk_n = profile_collect("traverse_plain")
+        profile_collect(None)
+        if dist is not None:
+            t = torch.tensor([pms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        out["plain"] = {"ms_per_step": pms / args.steps,
+                        "windows_per_s": world * args.windows / (pms / args.steps / 1e3),
+                        "kernel_ms": pk_ms / max(args.steps, 1)}
+        del offs
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    if "e2e" not in skip:
+        out["e2e"] = e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream,
+                             dist, world)
+
+    L.crt_profile_enable(0)
+    del fid, tid
+    torch.cuda.empty_cache()
+
+    # ---- bulk load ------------------------------------------------------------
+    if "build" not in skip:
+        out["build"] = build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world)
+    return out, boxes, windows
+
+
+def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, dist, world):
+    """Windows H2D from pinned host memory, query, all pairs D2H to pinned host
+    memory, per step, through the C ABI."""
+    import psutil
+    import torch
+    nwin = windows.n
+    pair_bytes = 8 * pairs
+    avail = psutil.virtual_memory().available
+    if pair_bytes * 1.5 > avail:
+        return {"value": None, "unit": "windows/s",
+                "skipped": f"host memory {avail / 1e9:.0f} GB < 1.5 x {pair_bytes / 1e9:.0f} GB of pairs"}
+    h_win = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+             for a in (windows.xmin, windows.ymin, windows.xmax, windows.ymax, windows.id)]
+    h_fid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
+    h_tid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
+    d_win = C.BBox.empty(nwin)
+    dst = [d_win.xmin, d_win.ymin, d_win.xmax, d_win.ymax, d_win.id]
+    h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+
+    def step():
+        for d, h in zip(dst, h_win):
+            d.copy_(h, non_blocking=True)
+        C.query_into(rt, sorted_box, d_win, fid, tid, res)
+        h_res.copy_(res, non_blocking=True)
+        h_fid.copy_(fid[:pairs], non_blocking=True)
+        h_tid.copy_(tid[:pairs], non_blocking=True)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    torch.cuda.synchronize()
+    r = C.read_result(h_res)
+    assert r["count"] == pairs and r["overflow"] == 0, r
+    ms = timed(step, args.steps, stream)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    h2d = sum(int(h.numel() * h.element_size()) for h in h_win)
+    return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * pairs + 64,
+            "ms_per_step": ms / args.steps, "path": "crt_query_into_f32 (persistent) via ctypes"}
+
+
+def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
+    import torch
+    from curtree_b200 import datasets as D
+    n = args.build_boxes
+    boxes = D.clustered_boxes(n, seed=2)
+    d_in = C.BBox.from_host(boxes)
+    del boxes
+    f = 10
+    rsz = C.tree_size(n, f)
+    out = C.BBox.empty(n)
+    rt = C.RTree(f)
+    ts = [torch.empty(rsz, dtype=dt, device="cuda") for dt in [torch.float32] * 4 + [torch.int32] * 2]
+    rt.s.xmin, rt.s.ymin, rt.s.xmax, rt.s.ymax, rt.s.pos, rt.s.len = [t.data_ptr() for t in ts]
+    ci, co = d_in.c(), out.c()
+    import ctypes
+    from curtree_b200 import _lib
+
+    def step():
+        _lib.check(L.crt_build_into_f32(ctypes.byref(ci), ctypes.byref(co), ctypes.byref(rt.s),
+                                        ctypes.c_void_p(stream.cuda_stream)), "build")
+
+    L.crt_profile_enable(1)
+    for _ in range(args.warmup):
+        step()
+    profile_collect(None)
+    ms = timed(step, args.steps, stream)
+    parts = {k: profile_collect(k)[0] / args.steps for k in ("encode", "sort_pass", "level")}
+    profile_collect(None)
+    L.crt_profile_enable(0)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    kern_ms = sum(parts.values())
+    b_build = 120 * n + 40 * rsz
+    strict = 40 * n + 24 * rsz
+    return {"metric": "build_boxes_per_s", "value": world * n / (ms / args.steps / 1e3),
+            "unit": "boxes/s", "ms_per_step": ms / args.steps, "kernel_ms": kern_ms,
+            "kernels_ms": parts, "fanout": f, "boxes": n, "r_sz": rsz,
+            "workload": "100M clustered boxes (1000 Gaussians + 10% uniform, log-normal sides, "
+                        "1% duplicates, 1% points), out-of-place crt_build_into_f32",
+            "roofline": {"bound": "hbm", "achieved": b_build / (kern_ms / 1e3) / 1e9,
+                         "peak": hbm_peak, "unit": "GB/s",
+                         "frac": b_build / (kern_ms / 1e3) / 1e9 / hbm_peak, "traffic": None,
+                         "peak_kind": peak_kind, "algorithmic_bytes": b_build,
+                         "bytes_model": "120 B/box + 40 B/node",
+                         "strict_io_frac": strict / (kern_ms / 1e3) / 1e9 / hbm_peak}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from curtree_b200 import datasets as D
+        boxes, windows = make_query_inputs(0, args.boxes, args.windows)
+        vals = []
+        samples = []
+        per_step = max(2.0, args.cpu_seconds / 2)
+        for i in range(args.warmup + args.steps):
+            r = cpu_reference_rate(boxes, windows, per_step, rng_seed=11 + i)
+            if i >= args.warmup:
+                vals.append(r["value"])
+                samples.append(r["sample"])
+        v = statistics.median(vals)
+        line = {"impl": "reference", "metric": "window_queries_per_s", "value": v,
+                "unit": "windows/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": query_config(args),
+                "cpu_baseline": {"value": v, "unit": "windows/s", "cores": r["cores"],
+                                 "kind": r["kind"], "sample": samples[-1]},
+                "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    out, boxes, windows = run_ours(args, rank, world, dist)
+    skip = set(s for s in args.skip.split(",") if s)
+    cpu = None
+    if rank == 0 and world == 1 and "cpu" not in skip:
+        cpu = cpu_reference_rate(boxes, windows, args.cpu_seconds)
+    if rank == 0:
+        p = out["persistent"]
+        line = {"metric": "window_queries_per_s", "value": p["windows_per_s"], "unit": "windows/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": p["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": query_config(args),
+                "roofline": out["roofline"], "cpu_baseline": cpu, "e2e": out.get("e2e"),
+                "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
+                "plain": out.get("plain"), "build": out.get("build"),
+                "workload_stats": out["workload_stats"],
+                "persistent_kernel_ms": p["kernel_ms"]}
+        if "plain" in out:
+            line["persistent_vs_plain"] = p["windows_per_s"] / out["plain"]["windows_per_s"]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def query_config(args):
+    return {"workload": f"{args.boxes // 10**6}M uniform boxes (side U[0,1e-3]) x "
+                        f"{args.windows // 1000}k mixed windows (side log-U[1e-5,1e-1], half on "
+                        f"box centres), fanout {args.fanout}, persistent graph-captured form",
+            "boxes": args.boxes, "windows": args.windows, "fanout": args.fanout,
+            "parallelism": "replicas (each GPU its own tree copy and window batch)",
+            "l2": "inputs larger than L2 (box SoA 200 MB, pair output tens of GB); no flush"}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,521 @@
+// Z-order bulk load (replaces build_rtree, src/rtree_bulkload_thrust.cuh:62-213).
+//
+// Pipeline, all on one stream, no host synchronisation until the end:
+//   1. encode      read the box SoA once (float4 loads where aligned), write the
+//                  flipped 32-bit Morton key and a 32-byte AoS copy of each box
+//                  (one DRAM sector, so the later random gather costs one
+//                  sector per box), and count all four 8-bit key digits.
+//   2. plan        one CTA: which digit passes are non-uniform (a uniform digit
+//                  leaves a stable order unchanged, so its pass is skipped) and
+//                  the global bucket start of every digit value.
+//   3. 4 x onesweep  stable LSD radix passes over (key, slot) with decoupled
+//                  look-back across tiles: one read and one write of the pairs
+//                  per pass.  The first active pass makes the slot values, the
+//                  last one writes only slots.
+//   4. leaf level  gather each sorted box from the AoS copy, write the permuted
+//                  SoA, and reduce every run of `fanout` boxes into its
+//                  leaf-parent node.
+//   5. upper levels  reduce runs of `fanout` nodes, level by level up to the root.
+// Node order, pos and len follow the reference exactly (root at 0, levels
+// downward, children contiguous, leaf-parent pos = R_sz + first slot).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+#include "profile.h"
+
+namespace crt {
+
+struct alignas(32) Box32 {
+  float4 mbr;  // xmin, ymin, xmax, ymax
+  int4 idp;    // id, 0, 0, 0
+};
+
+constexpr int kRadixBits = 8;
+constexpr int kSortThreads = 512;
+constexpr int kSortIpt = kSortTile / kSortThreads;  // 16 keys per thread
+constexpr int kSortWarps = kSortThreads / 32;
+static_assert(kBins == 1 << kRadixBits, "digit width");
+using BuildCtrl = SortCtrl;
+
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagIncl = 2ull << 62;
+
+// ---------------------------------------------------------------------------
+// 1. encode
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void encode_one(float a, float b, float c, float d, int id, int64_t i,
+                                           uint32_t* keys, Box32* aos, uint32_t (*sh)[kBins])
+{
+  uint32_t k = sort_key(a, b, c, d);
+  keys[i] = k;
+  Box32 bx;
+  bx.mbr = make_float4(a, b, c, d);
+  bx.idp = make_int4(id, 0, 0, 0);
+  aos[i] = bx;
+  atomicAdd(&sh[0][k & 0xFF], 1u);
+  atomicAdd(&sh[1][(k >> 8) & 0xFF], 1u);
+  atomicAdd(&sh[2][(k >> 16) & 0xFF], 1u);
+  atomicAdd(&sh[3][k >> 24], 1u);
+}
+
+template <bool kVec>
+__global__ void __launch_bounds__(256) encode_kernel(const float* __restrict__ xmin,
+                                                     const float* __restrict__ ymin,
+                                                     const float* __restrict__ xmax,
+                                                     const float* __restrict__ ymax,
+                                                     const int* __restrict__ id, int64_t n,
+                                                     uint32_t* __restrict__ keys,
+                                                     Box32* __restrict__ aos,
+                                                     uint32_t* __restrict__ hist)
+{
+  __shared__ uint32_t sh[4][kBins];
+  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  if (kVec) {
+    const int64_t n4 = n / 4;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n4; g += stride) {
+      float4 a = reinterpret_cast<const float4*>(xmin)[g];
+      float4 b = reinterpret_cast<const float4*>(ymin)[g];
+      float4 c = reinterpret_cast<const float4*>(xmax)[g];
+      float4 d = reinterpret_cast<const float4*>(ymax)[g];
+      int4 e = reinterpret_cast<const int4*>(id)[g];
+      encode_one(a.x, b.x, c.x, d.x, e.x, 4 * g + 0, keys, aos, sh);
+      encode_one(a.y, b.y, c.y, d.y, e.y, 4 * g + 1, keys, aos, sh);
+      encode_one(a.z, b.z, c.z, d.z, e.z, 4 * g + 2, keys, aos, sh);
+      encode_one(a.w, b.w, c.w, d.w, e.w, 4 * g + 3, keys, aos, sh);
+    }
+    for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+      encode_one(xmin[i], ymin[i], xmax[i], ymax[i], id[i], i, keys, aos, sh);
+  } else {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+      encode_one(xmin[i], ymin[i], xmax[i], ymax[i], id[i], i, keys, aos, sh);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) {
+    uint32_t v = (&sh[0][0])[i];
+    if (v) atomicAdd(&hist[i], v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. plan
+// ---------------------------------------------------------------------------
+__global__ void plan_kernel(const uint32_t* __restrict__ hist, int64_t n, BuildCtrl* ctrl)
+{
+  __shared__ int s_uniform[4];
+  if (threadIdx.x < 4) s_uniform[threadIdx.x] = 0;
+  __syncthreads();
+  // one warp per digit: exclusive scan of its 256 bins
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (w < 4) {
+    uint32_t carry = 0;
+    for (int c = 0; c < kBins; c += 32) {
+      uint32_t v = hist[w * kBins + c + l];
+      if ((int64_t)v == n) s_uniform[w] = 1;
+      uint32_t x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (l >= o) x += y;
+      }
+      ctrl->bucket_start[w * kBins + c + l] = (int)(carry + x - v);
+      carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int act = 0, na = 0;
+    for (int d = 0; d < 4; d++)
+      if (!s_uniform[d]) { act |= 1 << d; na++; }
+    ctrl->active = act;
+    ctrl->n_active = na;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. onesweep pass
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSortThreads, 2)
+    onesweep_kernel(int digit, SortBufs bufs, int64_t n, uint64_t* __restrict__ status,
+                    BuildCtrl* __restrict__ ctrl)
+{
+  extern __shared__ uint32_t smem[];
+  uint32_t* s_keys = smem;                       // kSortTile
+  uint32_t* s_vals = smem + kSortTile;           // kSortTile
+  uint32_t* s_whist = smem + 2 * kSortTile;      // kSortWarps * kBins
+  __shared__ int s_binstart[kBins];
+  __shared__ int s_gbase[kBins];
+  __shared__ int s_tile;
+  __shared__ int s_wsum[kBins / 32];
+
+  const int active = ctrl->active;
+  if (!((active >> digit) & 1)) return;
+  const int before = active & ((1 << digit) - 1);
+  const int parity = __popc(before) & 1;
+  const bool first = before == 0;
+  const bool last = (active >> (digit + 1)) == 0;
+  const uint32_t* __restrict__ src_k = bufs.keys[parity];
+  const uint32_t* __restrict__ src_v = bufs.vals[parity];
+  uint32_t* __restrict__ dst_k = bufs.keys[parity ^ 1];
+  uint32_t* __restrict__ dst_v = bufs.vals[parity ^ 1];
+  const int shift = digit * kRadixBits;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(&ctrl->tile_ctr[digit], 1);
+  for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) s_whist[i] = 0;
+  __syncthreads();
+  const int tile = s_tile;
+  const int64_t base = (int64_t)tile * kSortTile;
+  const int64_t wbase = base + (int64_t)warp * 32 * kSortIpt;
+
+  // load keys (warp-striped: item i of a lane is wbase + i*32 + lane)
+  uint32_t key[kSortIpt];
+  uint32_t rank[kSortIpt];
+#pragma unroll
+  for (int i = 0; i < kSortIpt; i++) {
+    int64_t g = wbase + i * 32 + lane;
+    key[i] = g < n ? src_k[g] : 0u;
+  }
+  // rank inside the warp, stably: rounds in order, lanes in order
+  uint32_t* wh = s_whist + warp * kBins;
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kSortIpt; i++) {
+    int64_t g = wbase + i * 32 + lane;
+    uint32_t dig = g < n ? (key[i] >> shift) & 0xFF : kBins;
+    uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    uint32_t old = dig < kBins ? wh[dig] : 0u;
+    __syncwarp();
+    if (dig < kBins && lane == (uint32_t)(__ffs(peers) - 1)) wh[dig] = old + __popc(peers);
+    __syncwarp();
+    rank[i] = old + __popc(peers & lt);
+  }
+  __syncthreads();
+  // per bin: exclusive over warps -> warp offsets; totals -> tile counts
+  int cnt = 0;
+  if (tid < kBins) {
+    int run = 0;
+    for (int w = 0; w < kSortWarps; w++) {
+      int c = (int)s_whist[w * kBins + tid];
+      s_whist[w * kBins + tid] = run;
+      run += c;
+    }
+    cnt = run;
+    // block exclusive scan of cnt over the 256 bins (8 warps)
+    int x = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_wsum[warp] = x;
+    s_binstart[tid] = x - cnt;  // partial, fixed below
+  }
+  __syncthreads();
+  if (tid < kBins) {
+    int add = 0;
+    for (int w = 0; w < warp; w++) add += s_wsum[w];
+    s_binstart[tid] += add;
+
+    // decoupled look-back for bin `tid`
+    uint64_t* st = status;
+    int excl = 0;
+    if (tile == 0) {
+      st_relaxed_u64(&st[tid], kFlagIncl | (uint32_t)cnt);
+    } else {
+      st_relaxed_u64(&st[(int64_t)tile * kBins + tid], kFlagAgg | (uint32_t)cnt);
+      int t = tile - 1;
+      uint32_t spins = 0;
+      while (true) {
+        uint64_t v = ld_relaxed_u64(&st[(int64_t)t * kBins + tid]);
+        uint64_t flag = v & (3ull << 62);
+        if (flag == 0) {
+          if (++spins > kSpinLimit || ld_relaxed_i32(&ctrl->error) != 0) {
+            raise_error(&ctrl->error, CRT_ERR_DEVICE_TIMEOUT);
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+          continue;
+        }
+        excl += (int)(uint32_t)v;
+        if (flag == kFlagIncl) break;
+        --t;
+      }
+      st_relaxed_u64(&st[(int64_t)tile * kBins + tid], kFlagIncl | (uint32_t)(excl + cnt));
+    }
+    s_gbase[tid] = ctrl->bucket_start[digit * kBins + tid] + excl - s_binstart[tid];
+  }
+  __syncthreads();
+
+  // stage keys (and slots) in tile order of their destination
+#pragma unroll
+  for (int i = 0; i < kSortIpt; i++) {
+    int64_t g = wbase + i * 32 + lane;
+    if (g < n) {
+      uint32_t dig = (key[i] >> shift) & 0xFF;
+      int pos = s_binstart[dig] + (int)s_whist[warp * kBins + dig] + (int)rank[i];
+      s_keys[pos] = key[i];
+      s_vals[pos] = first ? (uint32_t)g : src_v[g];
+    }
+  }
+  __syncthreads();
+  const int tile_n = (int)min((int64_t)kSortTile, n - base);
+  for (int j = tid; j < tile_n; j += kSortThreads) {
+    uint32_t k = s_keys[j];
+    int dst = s_gbase[(k >> shift) & 0xFF] + j;
+    if ((uint32_t)dst < (uint64_t)n) {
+      if (!last) dst_k[dst] = k;
+      dst_v[dst] = s_vals[j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4./5. level reductions
+// ---------------------------------------------------------------------------
+constexpr int kLevelThreads = 256;
+constexpr int kLevelChunk = 2048;  // children staged per round
+
+// Reduces runs of `fanout` consecutive children into parent nodes
+// (reduce_op, src/rtree_bulkload_thrust.cuh:38-50: min, min, max, max of the
+// MBR, first child index, child count).  kLeaf: children are the sorted boxes,
+// gathered from the AoS copy through the sorted slot order, and the permuted
+// SoA is written on the way; otherwise children are nodes at child_start.
+template <bool kLeaf>
+__global__ void __launch_bounds__(kLevelThreads)
+    level_kernel(int nodes_per_cta, int fanout, int64_t nchild, int64_t nparent,
+                 int64_t parent_start, int64_t pos_base,
+                 // leaf inputs/outputs
+                 const uint32_t* __restrict__ vals0, const uint32_t* __restrict__ vals1,
+                 const BuildCtrl* __restrict__ ctrl, const Box32* __restrict__ aos,
+                 float* __restrict__ oxmin, float* __restrict__ oymin,
+                 float* __restrict__ oxmax, float* __restrict__ oymax, int* __restrict__ oid,
+                 // node arrays
+                 float* __restrict__ nxmin, float* __restrict__ nymin,
+                 float* __restrict__ nxmax, float* __restrict__ nymax, int* __restrict__ npos,
+                 int* __restrict__ nlen, int64_t child_start)
+{
+  __shared__ float4 s_mbr[kLevelChunk];
+  const int64_t p0 = (int64_t)blockIdx.x * nodes_per_cta;
+  const int64_t p1 = min(nparent, p0 + nodes_per_cta);
+  if (p0 >= p1) return;
+  const int64_t c0 = p0 * fanout;
+  const int64_t c1 = min(nchild, p1 * fanout);
+  const uint32_t* sorted = nullptr;
+  if (kLeaf) {
+    int na = ctrl->n_active;
+    sorted = na == 0 ? nullptr : ((na & 1) ? vals1 : vals0);
+  }
+  // this thread's parent (if any) and its child range
+  const int64_t my = p0 + threadIdx.x;
+  const bool have = my < p1;
+  const int64_t my_c0 = my * fanout;
+  const int64_t my_c1 = min(nchild, my_c0 + fanout);
+  float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
+  bool init = false;
+  for (int64_t cb = c0; cb < c1; cb += kLevelChunk) {
+    const int64_t ce = min(c1, cb + (int64_t)kLevelChunk);
+    for (int64_t s = cb + threadIdx.x; s < ce; s += kLevelThreads) {
+      float4 m;
+      if (kLeaf) {
+        int64_t src = sorted ? (int64_t)sorted[s] : s;
+        if (src >= nchild) src = s;  // only reachable after a sort error (reported)
+        Box32 bx = aos[src];
+        m = bx.mbr;
+        oxmin[s] = m.x;
+        oymin[s] = m.y;
+        oxmax[s] = m.z;
+        oymax[s] = m.w;
+        oid[s] = bx.idp.x;
+      } else {
+        const int64_t i = child_start + s;
+        m = make_float4(nxmin[i], nymin[i], nxmax[i], nymax[i]);
+      }
+      s_mbr[s - cb] = m;
+    }
+    __syncthreads();
+    if (have) {
+      const int64_t lo = max(my_c0, cb), hi = min(my_c1, ce);
+      for (int64_t s = lo; s < hi; s++) {
+        float4 m = s_mbr[s - cb];
+        if (!init) {
+          a = m.x; b = m.y; c = m.z; d = m.w;
+          init = true;
+        } else {
+          a = fminf(a, m.x);
+          b = fminf(b, m.y);
+          c = fmaxf(c, m.z);
+          d = fmaxf(d, m.w);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (have) {
+    const int64_t o = parent_start + my;
+    nxmin[o] = a;
+    nymin[o] = b;
+    nxmax[o] = c;
+    nymax[o] = d;
+    npos[o] = (int)(pos_base + my_c0);
+    nlen[o] = (int)(my_c1 - my_c0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+int tree_levels(int64_t n, int fanout, std::vector<int64_t>& lv)
+{
+  lv.clear();
+  if (n < 1 || fanout < 2) return -1;
+  int64_t len = n;
+  while (len != 1) {
+    len = (len + fanout - 1) / fanout;
+    lv.push_back(len);
+  }
+  return (int)lv.size();
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+static int64_t sort_tiles(int64_t n) { return std::max<int64_t>(1, cdiv(n, kSortTile)); }
+
+size_t sort_zero_bytes(int64_t n)
+{
+  return sizeof(SortCtrl) + 4 * kBins * sizeof(uint32_t) +
+         (size_t)4 * sort_tiles(n) * kBins * sizeof(uint64_t);
+}
+SortCtrl* sort_ctrl(void* zero_block) { return (SortCtrl*)zero_block; }
+uint32_t* sort_hist(void* zero_block) { return (uint32_t*)((char*)zero_block + sizeof(SortCtrl)); }
+static uint64_t* sort_status(void* zero_block)
+{
+  return (uint64_t*)((char*)zero_block + sizeof(SortCtrl) + 4 * kBins * sizeof(uint32_t));
+}
+
+void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream)
+{
+  const int64_t ntiles = sort_tiles(n);
+  SortCtrl* ctrl = sort_ctrl(zero_block);
+  uint64_t* status = sort_status(zero_block);
+  plan_kernel<<<1, 128, 0, stream>>>(sort_hist(zero_block), n, ctrl);
+  const size_t smem = (2 * kSortTile + kSortWarps * kBins) * sizeof(uint32_t);
+  cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  for (int d = 0; d < 4; d++) {
+    ProfScope ps("sort_pass", stream);
+    onesweep_kernel<<<(unsigned)ntiles, kSortThreads, smem, stream>>>(
+        d, bufs, n, status + (size_t)d * ntiles * kBins, ctrl);
+  }
+  CRT_LAUNCHED(5);
+}
+
+// Builds the tree of `n` boxes.  in_* may alias out_* (in-place build).
+// Node arrays must hold R_sz entries.  Synchronises `stream` at the end and
+// reports device-side errors.
+int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
+               const float* in_ymax, const int* in_id, int64_t n, int fanout, float* out_xmin,
+               float* out_ymin, float* out_xmax, float* out_ymax, int* out_id, float* nxmin,
+               float* nymin, float* nxmax, float* nymax, int* npos, int* nlen,
+               cudaStream_t stream)
+{
+  std::vector<int64_t> lv;
+  if (tree_levels(n, fanout, lv) < 0)
+    return fail(CRT_ERR_INVALID_ARG, "build: need n >= 1 and fanout >= 2");
+  int64_t rsz = 0;
+  for (auto x : lv) rsz += x;
+  if (n + rsz > INT32_MAX)
+    return fail(CRT_ERR_INVALID_ARG, "build: n + R_sz exceeds the int32 pos range of RTREE");
+
+  // scratch: [ctrl | hist | status] (zeroed) then keys/vals/aos
+  const size_t zero_bytes = sort_zero_bytes(n);
+  const size_t kv_bytes = ((size_t)n * 4 + 255) / 256 * 256;
+  const size_t aos_bytes = (size_t)n * sizeof(Box32);
+  const size_t total = (zero_bytes + 255) / 256 * 256 + 4 * kv_bytes + aos_bytes + 256;
+  char* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&scratch, total, stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRT_ERR_OOM, "build: scratch allocation failed");
+  }
+  size_t off = (zero_bytes + 255) / 256 * 256;
+  BuildCtrl* ctrl = sort_ctrl(scratch);
+  uint32_t* hist = sort_hist(scratch);
+  SortBufs bufs;
+  bufs.keys[0] = (uint32_t*)(scratch + off); off += kv_bytes;
+  bufs.keys[1] = (uint32_t*)(scratch + off); off += kv_bytes;
+  bufs.vals[0] = (uint32_t*)(scratch + off); off += kv_bytes;
+  bufs.vals[1] = (uint32_t*)(scratch + off); off += kv_bytes;
+  Box32* aos = (Box32*)(scratch + off);
+
+  int rc = CRT_OK;
+  do {
+    if ((e = cudaMemsetAsync(scratch, 0, zero_bytes, stream)) != cudaSuccess) break;
+    const int sms = sm_count();
+    const bool vec = aligned16(in_xmin) && aligned16(in_ymin) && aligned16(in_xmax) &&
+                     aligned16(in_ymax) && aligned16(in_id);
+    int64_t work = vec ? cdiv(n, 4) : n;
+    int grid = (int)std::min<int64_t>(cdiv(work, 256), (int64_t)sms * 8);
+    if (grid < 1) grid = 1;
+    {
+    ProfScope ps("encode", stream);
+    if (vec)
+      encode_kernel<true><<<grid, 256, 0, stream>>>(in_xmin, in_ymin, in_xmax, in_ymax, in_id, n,
+                                                    bufs.keys[0], aos, hist);
+    else
+      encode_kernel<false><<<grid, 256, 0, stream>>>(in_xmin, in_ymin, in_xmax, in_ymax, in_id,
+                                                     n, bufs.keys[0], aos, hist);
+    }
+    CRT_LAUNCHED(1);
+    sort_passes(bufs, n, scratch, stream);
+
+    // leaf-parent level
+    int64_t parent_start = rsz;
+    int64_t child_start = 0, nchild = n;
+    for (size_t l = 0; l < lv.size(); l++) {
+      const int64_t np = lv[l];
+      parent_start -= np;
+      int npc = (int)std::max<int64_t>(1, std::min<int64_t>(kLevelThreads, kLevelChunk / fanout));
+      unsigned g = (unsigned)cdiv(np, npc);
+      ProfScope ps("level", stream);
+      if (l == 0)
+        level_kernel<true><<<g, kLevelThreads, 0, stream>>>(
+            npc, fanout, nchild, np, parent_start, rsz, bufs.vals[0], bufs.vals[1], ctrl, aos,
+            out_xmin, out_ymin, out_xmax, out_ymax, out_id, nxmin, nymin, nxmax, nymax, npos,
+            nlen, 0);
+      else
+        level_kernel<false><<<g, kLevelThreads, 0, stream>>>(
+            npc, fanout, nchild, np, parent_start, child_start, nullptr, nullptr, ctrl, nullptr,
+            nullptr, nullptr, nullptr, nullptr, nullptr, nxmin, nymin, nxmax, nymax, npos, nlen,
+            child_start);
+      CRT_LAUNCHED(1);
+      child_start = parent_start;
+      nchild = np;
+    }
+    if (lv.empty()) {
+      // one box, no nodes: the sorted box set is the input itself
+      if (out_xmin != in_xmin) {
+        cudaMemcpyAsync(out_xmin, in_xmin, 4, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(out_ymin, in_ymin, 4, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(out_xmax, in_xmax, 4, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(out_ymax, in_ymax, 4, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(out_id, in_id, 4, cudaMemcpyDeviceToDevice, stream);
+      }
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    int dev_err = 0;
+    if ((e = cudaMemcpyAsync(&dev_err, &ctrl->error, sizeof(int), cudaMemcpyDeviceToHost,
+                             stream)) != cudaSuccess)
+      break;
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) break;
+    if (dev_err) rc = fail(dev_err, "build: device-side wait timed out in the radix sort");
+  } while (0);
+  cudaFreeAsync(scratch, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "build");
+  return rc;
+}
+
+}  // namespace crt

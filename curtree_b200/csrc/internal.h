@@ -1,0 +1,56 @@
+// Internal host interfaces shared between the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace crt {
+
+// Radix-sort scratch shared by the box build and the window ordering.
+struct SortBufs {
+  uint32_t* keys[2];
+  uint32_t* vals[2];
+};
+
+constexpr int kBins = 256;
+constexpr int kSortTile = 8192;
+
+// Control block of one sort (int32 words, zero-initialised by the caller).
+struct SortCtrl {
+  int tile_ctr[4];  // per pass: next tile index
+  int error;        // first device error
+  int active;       // bit d: digit d is non-uniform
+  int n_active;     // number of active passes: the order is in vals[n_active & 1]
+  int pad[9];
+  int bucket_start[4 * kBins];
+};
+
+// Bytes of zero-initialised state a sort of n keys needs: SortCtrl, the four
+// digit histograms and the look-back status words (in that order).
+size_t sort_zero_bytes(int64_t n);
+// Enqueues plan + four onesweep passes; keys must be in bufs.keys[0] and the
+// histograms filled.  The sorted positions end in bufs.vals[n_active & 1]
+// (identity when no pass is active).
+void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream);
+uint32_t* sort_hist(void* zero_block);
+SortCtrl* sort_ctrl(void* zero_block);
+
+int tree_levels(int64_t n, int fanout, std::vector<int64_t>& lv);
+
+int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
+               const float* in_ymax, const int* in_id, int64_t n, int fanout, float* out_xmin,
+               float* out_ymin, float* out_xmax, float* out_ymax, int* out_id, float* nxmin,
+               float* nymin, float* nxmax, float* nymax, int* npos, int* nlen,
+               cudaStream_t stream);
+
+// Query entry used by the C ABI.
+int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
+               int32_t* fid, int32_t* tid, int64_t capacity, crt_query_result* d_result,
+               int64_t* d_offsets, const crt_query_opts& opts, cudaStream_t stream);
+int64_t query_capacity(int64_t pairs, const crt_query_opts& opts);
+
+}  // namespace crt

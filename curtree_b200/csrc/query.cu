@@ -1,0 +1,1093 @@
+// Batched window query (replaces bfs_frontier, src/rtree_bfs_frontier.cuh:292-529,
+// and bfs_thrust, src/rtree_bfs_thrust.cuh:59-256).
+//
+// Semantics kept from the reference: the root is never tested; a node whose
+// children are nodes passes on the children whose MBR intersects the window
+// (src/rtree_bfs_frontier.cuh:110-124); a leaf-parent (pos >= R_sz) tests its
+// boxes at slots [pos - R_sz, pos - R_sz + len) (count_hit/write_hit,
+// :191-289); a hit emits (fid = sorted box's id, tid = window index).
+//
+// Traversal: one warp per window.  The warp keeps its frontier in shared
+// memory as a stack of node indices.  Each step pops up to K = 32 / fanout
+// nodes (one child per lane, children read in SoA layout, coalesced), tests
+// the children, compacts the intersecting inner children back onto the stack
+// with a ballot/popc prefix, and emits leaf hits warp-collectively.  Popping
+// the top K entries and pushing shallower parents' children first keeps the
+// stack ordered by depth, so it never holds more than K*fanout entries per
+// level: (levels - 1) * K * fanout + 1 in total, which the host sizes exactly.
+//
+// Two forms:
+//   plain       one warp per window in input order, a count pass, an int64
+//               exclusive scan and a write pass: output grouped by window.
+//   persistent  #SM x occupancy CTAs; warps take windows from an atomic ticket
+//               in Morton order of the window centres (neighbouring windows
+//               share tree paths, so the tree stays in L2); the top tree levels
+//               are staged in shared memory with bulk async copies; hits go to
+//               4096-slot chunks a warp reserves with one atomic, and a
+//               compaction pass moves the tail of the array into the unused
+//               ends of each warp's last chunk so the output is dense.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+#include "profile.h"
+
+namespace crt {
+
+struct TreeView {
+  const float* __restrict__ nxmin;
+  const float* __restrict__ nymin;
+  const float* __restrict__ nxmax;
+  const float* __restrict__ nymax;
+  const int* __restrict__ npos;
+  const int* __restrict__ nlen;
+  int rsz;
+  int fanout;
+  const float* __restrict__ bxmin;
+  const float* __restrict__ bymin;
+  const float* __restrict__ bxmax;
+  const float* __restrict__ bymax;
+  const int* __restrict__ bid;
+  int nbox;
+};
+
+struct WindowView {
+  const float* __restrict__ xmin;
+  const float* __restrict__ ymin;
+  const float* __restrict__ xmax;
+  const float* __restrict__ ymax;
+  int64_t n;
+};
+
+// Device-side counters of one query (int64 words; zeroed before a launch).
+struct QueryCounters {
+  unsigned long long ticket;  // next window (persistent)
+  unsigned long long next;    // next unreserved output slot
+  unsigned long long hits;    // exact pair count
+  unsigned long long nholes;  // unused chunk ends recorded
+  int error;
+  int pad;
+  unsigned long long nq;      // window count (read by graph replays)
+};
+
+struct Hole {
+  long long start;
+  long long len;
+};
+
+// Top tree levels staged in shared memory (node index < n), or none.
+struct NodeCache {
+  const float* xmin;
+  const float* ymin;
+  const float* xmax;
+  const float* ymax;
+  const int* pos;
+  const int* len;
+  int n;
+};
+
+__device__ __forceinline__ void load_node_box(const TreeView& T, const NodeCache& C, int i,
+                                              float& a, float& b, float& c, float& d)
+{
+  if (i < C.n) {
+    a = C.xmin[i]; b = C.ymin[i]; c = C.xmax[i]; d = C.ymax[i];
+  } else {
+    a = __ldg(T.nxmin + i); b = __ldg(T.nymin + i); c = __ldg(T.nxmax + i); d = __ldg(T.nymax + i);
+  }
+}
+__device__ __forceinline__ void load_node_link(const TreeView& T, const NodeCache& C, int i,
+                                               int& p, int& l)
+{
+  if (i < C.n) {
+    p = C.pos[i]; l = C.len[i];
+  } else {
+    p = __ldg(T.npos + i); l = __ldg(T.nlen + i);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Emitters: warp-collective; `hit` and `id` are per lane.
+// ---------------------------------------------------------------------------
+struct CountEmit {
+  static constexpr bool kCountsTests = false;
+  long long hits = 0;
+  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
+};
+
+// Counts hits and the leaf boxes tested (workload statistics).
+struct StatEmit {
+  static constexpr bool kCountsTests = true;
+  long long hits = 0;
+  long long tested = 0;
+  __device__ __forceinline__ void begin(int) {}
+  __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
+  __device__ __forceinline__ void leaf_tests(int n) { tested += n; }
+};
+
+// Writes at precomputed per-window offsets (plain write pass).
+struct OffsetEmit {
+  static constexpr bool kCountsTests = false;
+  int32_t* fid;
+  int32_t* tid;
+  long long base;
+  long long cap;
+  int q;
+  __device__ __forceinline__ void begin(int qq) { q = qq; }
+  __device__ __forceinline__ void operator()(bool hit, int id)
+  {
+    uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    long long slot = base + __popc(m & lanemask_lt());
+    if (hit && slot < cap) {
+      fid[slot] = id;
+      tid[slot] = q;
+    }
+    base += __popc(m);
+  }
+};
+
+// Warp-reserved output chunks (persistent form).
+struct ChunkEmit {
+  static constexpr bool kCountsTests = false;
+  int32_t* fid;
+  int32_t* tid;
+  long long cap;
+  unsigned long long* next;
+  long long cur = 0, end = 0;
+  long long hits = 0;
+  int chunk;
+  int q;
+  __device__ __forceinline__ void begin(int qq) { q = qq; }
+  __device__ __forceinline__ void operator()(bool hit, int id)
+  {
+    uint32_t m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    const int nh = __popc(m);
+    const int r = __popc(m & lanemask_lt());
+    hits += nh;
+    long long slot;
+    if (cur + nh <= end) {
+      slot = cur + r;
+      cur += nh;
+    } else {
+      const long long left = end - cur;
+      unsigned long long nb = 0;
+      if (lane_id() == 0) nb = atomicAdd(next, (unsigned long long)chunk);
+      nb = __shfl_sync(0xffffffffu, nb, 0);
+      slot = r < left ? cur + r : (long long)nb + (r - left);
+      cur = (long long)nb + (nh - left);
+      end = (long long)nb + chunk;
+    }
+    if (hit && slot < cap) {
+      fid[slot] = id;
+      tid[slot] = q;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Warp traversal of one window
+// ---------------------------------------------------------------------------
+template <class Emit>
+__device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, int K,
+                                         int lane_g, int lane_c, float x1, float y1, float x2,
+                                         float y2, int* stack, int stack_cap, Emit& emit,
+                                         int* err)
+{
+  const int lane = (int)lane_id();
+  const uint32_t lt = lanemask_lt();
+  const int f = T.fanout;
+  if (T.rsz == 0) {
+    // one-box (or empty) tree: no nodes, test the boxes directly
+    for (int base = 0; base < T.nbox; base += 32) {
+      int s = base + lane;
+      bool hit = s < T.nbox &&
+                 intersects(x1, y1, x2, y2, T.bxmin[s], T.bymin[s], T.bxmax[s], T.bymax[s]);
+      if constexpr (Emit::kCountsTests) emit.leaf_tests(min(32, T.nbox - base));
+      emit(hit, hit ? T.bid[s] : 0);
+    }
+    return;
+  }
+  if (lane == 0) stack[0] = 0;
+  int sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    const int k = min(sp, K);
+    sp -= k;
+    // popped entries stack[sp .. sp+k): lower index = shallower; lane g holds entry g
+    int my_pos = 0, my_len = 0;
+    if (lane < k) load_node_link(T, C, stack[sp + lane], my_pos, my_len);
+    __syncwarp();
+    const int span = f <= 32 ? 32 : f;  // children covered per node group
+    for (int base = 0; base < span; base += 32) {
+      int g, c;
+      if (f <= 32) { g = lane_g; c = lane_c; }
+      else { g = 0; c = base + lane; }
+      const int gs = min(g, k - 1);
+      const int pos = __shfl_sync(0xffffffffu, my_pos, gs);
+      const int len = __shfl_sync(0xffffffffu, my_len, gs);
+      const bool valid = g < k && c < len;
+      const int child = pos + c;
+      bool hit = false, push = false;
+      int hid = 0;
+      if (valid) {
+        if (pos >= T.rsz) {
+          const int s = child - T.rsz;
+          if (s < T.nbox) {
+            hit = intersects(x1, y1, x2, y2, __ldg(T.bxmin + s), __ldg(T.bymin + s),
+                             __ldg(T.bxmax + s), __ldg(T.bymax + s));
+            if (hit) hid = __ldg(T.bid + s);
+          }
+        } else if (child < T.rsz) {
+          float a, b, cc, d;
+          load_node_box(T, C, child, a, b, cc, d);
+          push = intersects(x1, y1, x2, y2, a, b, cc, d);
+        }
+      }
+      if constexpr (Emit::kCountsTests)
+        emit.leaf_tests(__popc(__ballot_sync(0xffffffffu, valid && pos >= T.rsz && child - T.rsz < T.nbox)));
+      const uint32_t pm = __ballot_sync(0xffffffffu, push);
+      if (pm) {
+        const int np = __popc(pm);
+        if (sp + np > stack_cap) {
+          // cannot happen with the host-sized stack; never write past it
+          raise_error(err, CRT_ERR_NOT_SUPPORTED);
+          return;
+        }
+        if (push) stack[sp + __popc(pm & lt)] = child;
+        sp += np;
+      }
+      emit(hit, hid);
+    }
+    __syncwarp();
+  }
+}
+
+// Lane -> (node group, child) for fanout <= 32.
+__device__ __forceinline__ void lane_map(int f, int K, int& g, int& c)
+{
+  const int lane = (int)lane_id();
+  if (f <= 32) {
+    g = lane / f;
+    c = lane - g * f;
+    if (g >= K) { g = 32; c = 0; }
+  } else {
+    g = 0;
+    c = lane;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain form: count pass / write pass, one warp per window in input order
+// ---------------------------------------------------------------------------
+constexpr int kPlainWarps = 8;
+
+__global__ void __launch_bounds__(kPlainWarps * 32)
+    plain_count_kernel(TreeView T, WindowView W, int K, int stack_cap,
+                       long long* __restrict__ counts, QueryCounters* ctr)
+{
+  extern __shared__ int s_stack[];
+  const int warp = threadIdx.x >> 5;
+  const long long q = (long long)blockIdx.x * kPlainWarps + warp;
+  if (q >= W.n) return;
+  int lg, lc;
+  lane_map(T.fanout, K, lg, lc);
+  NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+  CountEmit emit;
+  traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
+           s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
+  if (lane_id() == 0) counts[q] = emit.hits;
+}
+
+__global__ void __launch_bounds__(kPlainWarps * 32)
+    plain_write_kernel(TreeView T, WindowView W, int K, int stack_cap,
+                       const long long* __restrict__ offsets, int32_t* fid, int32_t* tid,
+                       long long cap, QueryCounters* ctr)
+{
+  extern __shared__ int s_stack[];
+  const int warp = threadIdx.x >> 5;
+  const long long q = (long long)blockIdx.x * kPlainWarps + warp;
+  if (q >= W.n) return;
+  if (offsets[W.n] > cap) return;  // overflow: the host reports the required size
+  int lg, lc;
+  lane_map(T.fanout, K, lg, lc);
+  NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+  OffsetEmit emit{fid, tid, offsets[q], cap, (int)q};
+  traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
+           s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
+}
+
+__global__ void __launch_bounds__(kPlainWarps * 32)
+    stats_kernel(TreeView T, WindowView W, int K, int stack_cap, long long* __restrict__ hits,
+                 long long* __restrict__ tested, unsigned long long* __restrict__ totals,
+                 QueryCounters* ctr)
+{
+  extern __shared__ int s_stack[];
+  const int warp = threadIdx.x >> 5;
+  const long long q = (long long)blockIdx.x * kPlainWarps + warp;
+  if (q >= W.n) return;
+  int lg, lc;
+  lane_map(T.fanout, K, lg, lc);
+  NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+  StatEmit emit;
+  traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
+           s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
+  if (lane_id() == 0) {
+    if (hits) hits[q] = emit.hits;
+    if (tested) tested[q] = emit.tested;
+    atomicAdd(&totals[0], (unsigned long long)emit.hits);
+    atomicAdd(&totals[1], (unsigned long long)emit.tested);
+  }
+}
+
+// int64 exclusive scan (counts -> offsets[0..n]), three kernels
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ long long block_incl_scan(long long v, long long* s_warp)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
+  }
+  if (lane == 31) s_warp[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    long long w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_warp[lane] = w;
+  }
+  __syncthreads();
+  if (warp > 0) v += s_warp[warp - 1];
+  __syncthreads();
+  return v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_block_sums(const long long* __restrict__ in, long long n, long long* __restrict__ sums)
+{
+  __shared__ long long s_warp[32];
+  long long i = (long long)blockIdx.x * kScanThreads + threadIdx.x;
+  long long v = i < n ? in[i] : 0;
+  v = block_incl_scan(v, s_warp);
+  if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_sums_kernel(long long* __restrict__ sums, long long nb)
+{
+  __shared__ long long s_warp[32];
+  __shared__ long long s_tot;
+  long long carry = 0;
+  for (long long b0 = 0; b0 < nb; b0 += kScanThreads) {
+    long long i = b0 + threadIdx.x;
+    long long v = i < nb ? sums[i] : 0;
+    long long x = block_incl_scan(v, s_warp);
+    if (i < nb) sums[i] = carry + x - v;  // exclusive
+    if (threadIdx.x == kScanThreads - 1) s_tot = x;
+    __syncthreads();
+    carry += s_tot;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    scan_apply_kernel(const long long* __restrict__ in, long long n,
+                      const long long* __restrict__ sums, long long* __restrict__ out)
+{
+  __shared__ long long s_warp[32];
+  long long i = (long long)blockIdx.x * kScanThreads + threadIdx.x;
+  long long v = i < n ? in[i] : 0;
+  long long x = block_incl_scan(v, s_warp);
+  long long base = sums[blockIdx.x];
+  if (i < n) out[i] = base + x - v;
+  if (i == n - 1) out[n] = base + x;
+}
+
+// Writes the result block of a plain query.
+__global__ void plain_result_kernel(const long long* __restrict__ offsets, long long n,
+                                    long long cap, QueryCounters* ctr, crt_query_result* res)
+{
+  long long total = n > 0 ? offsets[n] : 0;
+  res->required = total;
+  res->overflow = total > cap ? 1 : 0;
+  res->count = total > cap ? 0 : total;
+  res->error = ctr->error;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent form
+// ---------------------------------------------------------------------------
+struct PersistParams {
+  TreeView T;
+  WindowView W;
+  const uint32_t* order0;  // sorted window order candidates (vals[0], vals[1])
+  const uint32_t* order1;
+  const SortCtrl* sort_ctrl;  // n_active picks the buffer; null: input order
+  int K;
+  int stack_cap;
+  int stage_n;  // nodes staged in shared memory (multiple of 4), 0 = none
+  int chunk;
+  int32_t* fid;
+  int32_t* tid;
+  long long cap;
+  QueryCounters* ctr;
+  Hole* holes;
+  long long max_holes;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__global__ void __launch_bounds__(256)
+    persistent_kernel(PersistParams P)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) unsigned long long s_mbar;
+  __shared__ int s_stage_ok;
+  const int warps = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5;
+  // layout: [staged nodes: 6 arrays x stage_n x 4 B][stacks: warps x stack_cap x 4 B]
+  float* c_xmin = (float*)smem_raw;
+  float* c_ymin = c_xmin + P.stage_n;
+  float* c_xmax = c_ymin + P.stage_n;
+  float* c_ymax = c_xmax + P.stage_n;
+  int* c_pos = (int*)(c_ymax + P.stage_n);
+  int* c_len = c_pos + P.stage_n;
+  int* stacks = c_len + P.stage_n;
+  NodeCache C{c_xmin, c_ymin, c_xmax, c_ymax, c_pos, c_len, 0};
+
+  if (P.stage_n > 0) {
+    // bulk async copies of the top levels into shared memory, one mbarrier
+    const uint32_t bar = smem_addr(&s_mbar);
+    const uint32_t bytes = (uint32_t)P.stage_n * 4u;
+    if (threadIdx.x == 0) {
+      s_stage_ok = 1;
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                   "r"(6u * bytes)
+                   : "memory");
+      const void* src[6] = {P.T.nxmin, P.T.nymin, P.T.nxmax, P.T.nymax, P.T.npos, P.T.nlen};
+      void* dst[6] = {c_xmin, c_ymin, c_xmax, c_ymax, c_pos, c_len};
+      for (int a = 0; a < 6; a++)
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                "r"(smem_addr(dst[a])),
+            "l"(src[a]), "r"(bytes), "r"(bar)
+            : "memory");
+    }
+    // bounded wait for phase 0 (twice the usual limit: after a timeout the
+    // copies must not still be landing when the CTA leaves)
+    uint32_t done = 0;
+    for (uint32_t spin = 0; spin < 2 * kSpinLimit; spin++) {
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+      if (done) break;
+    }
+    if (!done) {
+      if (threadIdx.x == 0) s_stage_ok = 0;
+      raise_error(&P.ctr->error, CRT_ERR_DEVICE_TIMEOUT);
+    }
+    __syncthreads();
+    if (!s_stage_ok) return;
+    C.n = P.stage_n;
+  }
+
+  int* stack = stacks + warp * P.stack_cap;
+  int lg, lc;
+  lane_map(P.T.fanout, P.K, lg, lc);
+  const uint32_t* order = nullptr;
+  if (P.sort_ctrl) {
+    const int na = P.sort_ctrl->n_active;
+    order = na == 0 ? nullptr : ((na & 1) ? P.order1 : P.order0);
+  }
+  const long long nq = (long long)P.ctr->nq;
+  ChunkEmit emit;
+  emit.fid = P.fid;
+  emit.tid = P.tid;
+  emit.cap = P.cap;
+  emit.next = &P.ctr->next;
+  emit.chunk = P.chunk;
+  (void)warps;
+  while (true) {
+    unsigned long long t = 0;
+    if (lane_id() == 0) t = atomicAdd(&P.ctr->ticket, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if ((long long)t >= nq) break;
+    int q = order ? (int)order[t] : (int)t;
+    if (q < 0 || (long long)q >= nq) q = (int)t;  // only after a sort error (reported)
+    emit.begin(q);
+    traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
+             P.stack_cap, emit, &P.ctr->error);
+  }
+  if (lane_id() == 0) {
+    if (emit.hits) atomicAdd(&P.ctr->hits, (unsigned long long)emit.hits);
+    if (emit.end > emit.cur) {
+      unsigned long long h = atomicAdd(&P.ctr->nholes, 1ull);
+      if ((long long)h < P.max_holes) {
+        P.holes[h].start = emit.cur;
+        P.holes[h].len = emit.end - emit.cur;
+      } else {
+        raise_error(&P.ctr->error, CRT_ERR_NOT_SUPPORTED);
+      }
+    }
+  }
+}
+
+// Sorts the recorded holes by start (rank by counting: the list is short).
+__global__ void hole_sort_kernel(const Hole* __restrict__ holes, Hole* __restrict__ sorted,
+                                 const QueryCounters* __restrict__ ctr, long long max_holes)
+{
+  const long long nh = min((long long)ctr->nholes, max_holes);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nh;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = holes[i].start;
+    long long r = 0;
+    for (long long j = 0; j < nh; j++) r += holes[j].start < s;
+    sorted[r] = holes[i];
+  }
+}
+
+// Exclusive prefix of the sorted hole lengths (one CTA).
+__global__ void __launch_bounds__(kScanThreads)
+    hole_prefix_kernel(const Hole* __restrict__ sorted, long long* __restrict__ cum,
+                       const QueryCounters* __restrict__ ctr, long long max_holes)
+{
+  __shared__ long long s_warp[32];
+  __shared__ long long s_tot;
+  const long long nh = min((long long)ctr->nholes, max_holes);
+  long long carry = 0;
+  for (long long b0 = 0; b0 < nh; b0 += kScanThreads) {
+    long long i = b0 + threadIdx.x;
+    long long v = i < nh ? sorted[i].len : 0;
+    long long x = block_incl_scan(v, s_warp);
+    if (i < nh) cum[i] = carry + x - v;
+    if (threadIdx.x == kScanThreads - 1) s_tot = x;
+    __syncthreads();
+    carry += s_tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) cum[nh] = carry;
+}
+
+// Hole slots in [0, x): cum[i] + min(x - st[i], len[i]) for the last hole
+// starting before x.
+__device__ __forceinline__ long long holes_below(const Hole* h, const long long* cum, long long nh,
+                                                 long long x)
+{
+  long long lo = 0, hi = nh;  // first hole with start >= x
+  while (lo < hi) {
+    long long m = (lo + hi) >> 1;
+    if (h[m].start < x) lo = m + 1; else hi = m;
+  }
+  if (lo == 0) return 0;
+  const long long i = lo - 1;
+  return cum[i] + min(x - h[i].start, h[i].len);
+}
+
+// Moves every pair stored at or above `hits` into the holes below it, so the
+// output is dense [0, hits); then writes the result block.
+__global__ void compact_kernel(const Hole* __restrict__ h, const long long* __restrict__ cum,
+                               QueryCounters* __restrict__ ctr, long long max_holes,
+                               int32_t* fid, int32_t* tid, long long cap,
+                               crt_query_result* __restrict__ res)
+{
+  const long long nh = min((long long)ctr->nholes, max_holes);
+  const long long T = (long long)ctr->hits;
+  const long long R = (long long)ctr->next;
+  const bool overflow = R > cap;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    res->required = T;
+    res->overflow = overflow ? 1 : 0;
+    res->count = overflow ? 0 : T;
+    res->error = ctr->error;
+  }
+  if (overflow || ctr->error || nh == 0) return;
+  const long long below_T = holes_below(h, cum, nh, T);
+  for (long long s = T + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < R;
+       s += (long long)gridDim.x * blockDim.x) {
+    // inside a hole?
+    long long lo = 0, hi = nh;
+    while (lo < hi) {
+      long long m = (lo + hi) >> 1;
+      if (h[m].start <= s) lo = m + 1; else hi = m;
+    }
+    if (lo > 0 && s < h[lo - 1].start + h[lo - 1].len) continue;
+    const long long r = (s - T) - (holes_below(h, cum, nh, s) - below_T);
+    // r-th hole slot below T: last hole with cum <= r
+    long long a = 0, b = nh;
+    while (b - a > 1) {
+      long long m = (a + b) >> 1;
+      if (cum[m] <= r) a = m; else b = m;
+    }
+    const long long dst = h[a].start + (r - cum[a]);
+    if (dst < T && dst >= 0) {
+      fid[dst] = fid[s];
+      tid[dst] = tid[s];
+    }
+  }
+}
+
+// Window keys (same Morton key as the boxes) and digit histograms.
+__global__ void window_key_kernel(WindowView W, uint32_t* __restrict__ keys,
+                                  uint32_t* __restrict__ hist)
+{
+  __shared__ uint32_t sh[4][kBins];
+  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < W.n;
+       i += (long long)gridDim.x * blockDim.x) {
+    uint32_t k = sort_key(W.xmin[i], W.ymin[i], W.xmax[i], W.ymax[i]);
+    keys[i] = k;
+    atomicAdd(&sh[0][k & 0xFF], 1u);
+    atomicAdd(&sh[1][(k >> 8) & 0xFF], 1u);
+    atomicAdd(&sh[2][(k >> 16) & 0xFF], 1u);
+    atomicAdd(&sh[3][k >> 24], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) {
+    uint32_t v = (&sh[0][0])[i];
+    if (v) atomicAdd(&hist[i], v);
+  }
+}
+
+__global__ void set_nq_kernel(QueryCounters* ctr, long long nq) { ctr->nq = (unsigned long long)nq; }
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static TreeView make_view(const crt_rtree_f32& rt, const crt_bbox_f32& rb)
+{
+  TreeView T;
+  T.nxmin = rt.xmin; T.nymin = rt.ymin; T.nxmax = rt.xmax; T.nymax = rt.ymax;
+  T.npos = rt.pos; T.nlen = rt.len; T.rsz = rt.sz; T.fanout = rt.fanout;
+  T.bxmin = rb.xmin; T.bymin = rb.ymin; T.bxmax = rb.xmax; T.bymax = rb.ymax; T.bid = rb.id;
+  T.nbox = rb.sz;
+  return T;
+}
+
+// Number of levels of a tree with R_sz nodes over nbox boxes at this fanout
+// (1 when the root is the only level).
+static int levels_of(int64_t nbox, int fanout)
+{
+  std::vector<int64_t> lv;
+  int L = tree_levels(std::max<int64_t>(nbox, 1), std::max(fanout, 2), lv);
+  return std::max(L, 1);
+}
+
+struct TraversalShape {
+  int K;
+  int stack_cap;
+};
+
+static TraversalShape traversal_shape(int64_t nbox, int fanout)
+{
+  const int L = levels_of(nbox, fanout);
+  TraversalShape s;
+  s.K = fanout <= 32 ? std::max(1, 32 / fanout) : 1;
+  // at most K*fanout entries per pushed level (levels 1 .. L-1), plus the root
+  s.stack_cap = (L - 1) * s.K * fanout + 1;
+  s.stack_cap = (s.stack_cap + 31) / 32 * 32;
+  return s;
+}
+
+constexpr int kPersistThreads = 256;
+constexpr int kDefaultChunk = 4096;
+constexpr int kStageMaxNodes = 2048;
+
+static int persistent_grid(size_t smem)
+{
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel, kPersistThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * sm_count();
+}
+
+int64_t query_capacity(int64_t pairs, const crt_query_opts& o)
+{
+  if (o.mode == CRT_QUERY_PLAIN) return pairs;
+  const int chunk = o.chunk > 0 ? o.chunk : kDefaultChunk;
+  // every resident warp may leave one partly used chunk
+  const int64_t warps = (int64_t)sm_count() * 8 * (kPersistThreads / 32);
+  return pairs + warps * chunk;
+}
+
+struct PersistScratch {
+  QueryCounters* ctr;
+  Hole* holes;
+  Hole* sorted;
+  long long* cum;
+  void* sort_zero;
+  SortBufs bufs;
+  long long max_holes;
+  size_t bytes;
+};
+
+static size_t persist_scratch_bytes(int64_t max_nq, long long max_holes, bool sort)
+{
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  size_t b = al(sizeof(QueryCounters)) + 2 * al(sizeof(Hole) * max_holes) +
+             al(sizeof(long long) * (max_holes + 1));
+  if (sort) b += al(sort_zero_bytes(max_nq)) + 4 * al(4 * (size_t)std::max<int64_t>(max_nq, 1));
+  return b;
+}
+
+static void persist_scratch_carve(char* base, int64_t max_nq, long long max_holes, bool sort,
+                                  PersistScratch& S)
+{
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  size_t off = 0;
+  S.ctr = (QueryCounters*)(base + off); off += al(sizeof(QueryCounters));
+  S.holes = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
+  S.sorted = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
+  S.cum = (long long*)(base + off); off += al(sizeof(long long) * (max_holes + 1));
+  S.sort_zero = nullptr;
+  if (sort) {
+    S.sort_zero = base + off; off += al(sort_zero_bytes(max_nq));
+    size_t kv = al(4 * (size_t)std::max<int64_t>(max_nq, 1));
+    S.bufs.keys[0] = (uint32_t*)(base + off); off += kv;
+    S.bufs.keys[1] = (uint32_t*)(base + off); off += kv;
+    S.bufs.vals[0] = (uint32_t*)(base + off); off += kv;
+    S.bufs.vals[1] = (uint32_t*)(base + off); off += kv;
+  }
+  S.max_holes = max_holes;
+  S.bytes = off;
+}
+
+// Enqueues one persistent query (no host synchronisation).  `nq_dev` is read
+// from S.ctr->nq, which the caller sets (set_nq_kernel) before.
+static void enqueue_persistent(const TreeView& T, const WindowView& W, int64_t max_nq,
+                               const PersistScratch& S, bool sort, int stage_n, int32_t* fid,
+                               int32_t* tid, long long cap, int chunk, crt_query_result* res,
+                               cudaStream_t stream, cudaEvent_t ev0 = nullptr,
+                               cudaEvent_t ev1 = nullptr)
+{
+  const TraversalShape sh = traversal_shape(T.nbox, T.fanout);
+  // counters (keep nq) and the sort's zeroed block
+  cudaMemsetAsync(S.ctr, 0, offsetof(QueryCounters, nq), stream);
+  const int sms = sm_count();
+  if (sort && max_nq > 0) {
+    cudaMemsetAsync(S.sort_zero, 0, sort_zero_bytes(max_nq), stream);
+    int g = (int)std::min<int64_t>(cdiv(max_nq, 256), (int64_t)sms * 4);
+    window_key_kernel<<<std::max(g, 1), 256, 0, stream>>>(W, S.bufs.keys[0], sort_hist(S.sort_zero));
+    sort_passes(S.bufs, W.n, S.sort_zero, stream);
+    CRT_LAUNCHED(1);
+  }
+  PersistParams P;
+  P.T = T;
+  P.W = W;
+  P.order0 = S.bufs.vals[0];
+  P.order1 = S.bufs.vals[1];
+  P.sort_ctrl = sort ? sort_ctrl(S.sort_zero) : nullptr;
+  P.K = sh.K;
+  P.stack_cap = sh.stack_cap;
+  P.stage_n = stage_n;
+  P.chunk = chunk;
+  P.fid = fid;
+  P.tid = tid;
+  P.cap = cap;
+  P.ctr = S.ctr;
+  P.holes = S.holes;
+  P.max_holes = S.max_holes;
+  const size_t smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
+  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int grid = persistent_grid(smem);
+  {
+    ProfScope ps("traverse_persistent", stream);
+    if (ev0) cudaEventRecord(ev0, stream);
+    persistent_kernel<<<grid, kPersistThreads, smem, stream>>>(P);
+    if (ev1) cudaEventRecord(ev1, stream);
+  }
+  hole_sort_kernel<<<std::max(1, (int)cdiv(S.max_holes, 256)), 256, 0, stream>>>(
+      S.holes, S.sorted, S.ctr, S.max_holes);
+  hole_prefix_kernel<<<1, kScanThreads, 0, stream>>>(S.sorted, S.cum, S.ctr, S.max_holes);
+  compact_kernel<<<sms * 4, 256, 0, stream>>>(S.sorted, S.cum, S.ctr, S.max_holes, fid, tid,
+                                              cap, res);
+  CRT_LAUNCHED(4);
+}
+
+static int stage_nodes_for(const crt_rtree_f32& rt, bool want)
+{
+  if (!want || rt.sz <= 0) return 0;
+  const void* arrs[6] = {rt.xmin, rt.ymin, rt.xmax, rt.ymax, rt.pos, rt.len};
+  for (auto p : arrs)
+    if (((uintptr_t)p & 15u) != 0) return 0;
+  int n = std::min(rt.sz, kStageMaxNodes);
+  // whole levels only, counted from the root: nodes [0, n)
+  return n & ~3;
+}
+
+static long long max_holes_for(size_t smem)
+{
+  return (long long)persistent_grid(smem) * (kPersistThreads / 32);
+}
+
+int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
+               int32_t* fid, int32_t* tid, int64_t capacity, crt_query_result* d_result,
+               int64_t* d_offsets, const crt_query_opts& opts, cudaStream_t stream)
+{
+  if (!d_result) return fail(CRT_ERR_INVALID_ARG, "query: result block is required");
+  if (qbox.sz < 0 || rbox.sz < 0 || rt.sz < 0)
+    return fail(CRT_ERR_INVALID_ARG, "query: negative size");
+  if (rt.sz > 0 && rt.fanout < 2) return fail(CRT_ERR_INVALID_ARG, "query: fanout < 2");
+  if (capacity > 0 && (!fid || !tid)) return fail(CRT_ERR_INVALID_ARG, "query: null output");
+  const TreeView T = make_view(rt, rbox);
+  WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};
+  const int64_t nq = qbox.sz;
+  const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
+  const int sms = sm_count();
+
+  if (opts.mode == CRT_QUERY_PLAIN) {
+    // scratch: counters, counts, block sums (+ offsets when the caller gave none)
+    const int64_t nb = std::max<int64_t>(1, cdiv(nq, kScanThreads));
+    size_t bytes = 256 + 8 * (size_t)std::max<int64_t>(nq, 1) + 8 * (size_t)nb + 256 +
+                   (d_offsets ? 0 : 8 * (size_t)(nq + 1) + 256);
+    char* scr = nullptr;
+    if (cudaMallocAsync((void**)&scr, bytes, stream) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CRT_ERR_OOM, "query: scratch allocation failed");
+    }
+    QueryCounters* ctr = (QueryCounters*)scr;
+    long long* counts = (long long*)(scr + 256);
+    long long* sums = counts + std::max<int64_t>(nq, 1);
+    long long* offsets = d_offsets ? (long long*)d_offsets : sums + nb + 32;
+    cudaMemsetAsync(ctr, 0, sizeof(QueryCounters), stream);
+    cudaMemsetAsync(offsets, 0, 8, stream);
+    const size_t smem = (size_t)kPlainWarps * sh.stack_cap * 4;
+    cudaFuncSetAttribute(plain_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(plain_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (nq > 0) {
+      const unsigned g = (unsigned)cdiv(nq, kPlainWarps);
+      {
+        ProfScope ps("traverse_plain", stream);
+        plain_count_kernel<<<g, kPlainWarps * 32, smem, stream>>>(T, W, sh.K, sh.stack_cap, counts,
+                                                                  ctr);
+      }
+      scan_block_sums<<<(unsigned)nb, kScanThreads, 0, stream>>>(counts, nq, sums);
+      scan_sums_kernel<<<1, kScanThreads, 0, stream>>>(sums, nb);
+      scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, stream>>>(counts, nq, sums, offsets);
+      {
+        ProfScope ps("traverse_plain", stream);
+        plain_write_kernel<<<g, kPlainWarps * 32, smem, stream>>>(T, W, sh.K, sh.stack_cap,
+                                                                  offsets, fid, tid, capacity, ctr);
+      }
+      CRT_LAUNCHED(5);
+    }
+    plain_result_kernel<<<1, 1, 0, stream>>>(offsets, nq, capacity, ctr, d_result);
+    CRT_LAUNCHED(1);
+    cudaFreeAsync(scr, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "query (plain)");
+    return CRT_OK;
+  }
+
+  // persistent
+  const bool sort = opts.sort_windows != 0 && nq > 1;
+  const int stage_n = stage_nodes_for(rt, opts.stage_levels != 0);
+  const int chunk = opts.chunk >= 64 ? opts.chunk : kDefaultChunk;
+  const size_t smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
+  if (smem > 200 * 1024) return fail(CRT_ERR_NOT_SUPPORTED, "query: traversal stack too large");
+  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long max_holes = max_holes_for(smem);
+  const size_t bytes = persist_scratch_bytes(nq, max_holes, sort);
+  char* scr = nullptr;
+  if (cudaMallocAsync((void**)&scr, bytes, stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRT_ERR_OOM, "query: scratch allocation failed");
+  }
+  PersistScratch S;
+  persist_scratch_carve(scr, nq, max_holes, sort, S);
+  set_nq_kernel<<<1, 1, 0, stream>>>(S.ctr, nq);
+  CRT_LAUNCHED(1);
+  enqueue_persistent(T, W, nq, S, sort, stage_n, fid, tid, capacity, chunk, d_result, stream);
+  cudaFreeAsync(scr, stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "query (persistent)");
+  (void)sms;
+  return CRT_OK;
+}
+
+int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
+                int64_t* d_hits, int64_t* d_tested, int64_t* h_totals, cudaStream_t stream)
+{
+  const TreeView T = make_view(rt, rbox);
+  WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};
+  const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
+  char* scr = nullptr;
+  if (cudaMallocAsync((void**)&scr, 512, stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRT_ERR_OOM, "query_stats: scratch allocation failed");
+  }
+  QueryCounters* ctr = (QueryCounters*)scr;
+  unsigned long long* tot = (unsigned long long*)(scr + 256);
+  cudaMemsetAsync(scr, 0, 512, stream);
+  const size_t smem = (size_t)kPlainWarps * sh.stack_cap * 4;
+  cudaFuncSetAttribute(stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (qbox.sz > 0) {
+    stats_kernel<<<(unsigned)cdiv(qbox.sz, kPlainWarps), kPlainWarps * 32, smem, stream>>>(
+        T, W, sh.K, sh.stack_cap, (long long*)d_hits, (long long*)d_tested, tot, ctr);
+    CRT_LAUNCHED(1);
+  }
+  unsigned long long h[2] = {0, 0};
+  int err = 0;
+  cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, stream);
+  cudaMemcpyAsync(&err, &ctr->error, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  cudaFreeAsync(scr, stream);
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(e, "query_stats");
+  if (err) return fail(err, "query_stats: device-side error");
+  if (h_totals) {
+    h_totals[0] = (int64_t)h[0];
+    h_totals[1] = (int64_t)h[1];
+  }
+  return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent plan captured in a CUDA graph
+// ---------------------------------------------------------------------------
+struct Plan {
+  TreeView T;
+  WindowView W;
+  int64_t max_nq;
+  PersistScratch S;
+  char* scratch = nullptr;
+  bool sort;
+  int stage_n;
+  int chunk;
+  int32_t* fid;
+  int32_t* tid;
+  long long cap;
+  crt_query_result* res;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // kernel pair, replay pair
+};
+
+int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
+                int64_t max_nq, int32_t* fid, int32_t* tid, int64_t capacity,
+                crt_query_result* res, const crt_query_opts& opts, cudaStream_t stream,
+                void** out)
+{
+  if (!res || max_nq < 0) return fail(CRT_ERR_INVALID_ARG, "plan: bad arguments");
+  Plan* p = new Plan();
+  p->T = make_view(rt, rbox);
+  p->W = WindowView{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, max_nq};
+  p->max_nq = max_nq;
+  p->sort = opts.sort_windows != 0 && max_nq > 1;
+  p->stage_n = stage_nodes_for(rt, opts.stage_levels != 0);
+  p->chunk = opts.chunk >= 64 ? opts.chunk : kDefaultChunk;
+  p->fid = fid;
+  p->tid = tid;
+  p->cap = capacity;
+  p->res = res;
+  const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
+  const size_t smem = (size_t)p->stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
+  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long max_holes = max_holes_for(smem);
+  const size_t bytes = persist_scratch_bytes(max_nq, max_holes, p->sort);
+  if (cudaMalloc((void**)&p->scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete p;
+    return fail(CRT_ERR_OOM, "plan: scratch allocation failed");
+  }
+  persist_scratch_carve(p->scratch, max_nq, max_holes, p->sort, p->S);
+  cudaMemsetAsync(p->S.ctr, 0, sizeof(QueryCounters), stream);
+  set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
+  // capture on a private stream
+  cudaStream_t cs;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(p->scratch);
+    delete p;
+    return cuda_fail(cudaGetLastError(), "plan: stream");
+  }
+  if (profiling())
+    for (auto& ev : p->ev) cudaEventCreate(&ev);
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    // a window-sorting plan orders exactly max_nq windows, so it only runs
+    // with nq == max_nq (plan_set_nq enforces it); without sorting the
+    // kernel reads the live count from ctr->nq
+    enqueue_persistent(p->T, p->W, max_nq, p->S, p->sort, p->stage_n, fid, tid, capacity,
+                       p->chunk, res, cs, p->ev[0], p->ev[1]);
+    e = cudaStreamEndCapture(cs, &p->graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  cudaStreamSynchronize(stream);
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) {
+    if (p->graph) cudaGraphDestroy(p->graph);
+    cudaFree(p->scratch);
+    delete p;
+    return cuda_fail(e, "plan: graph capture");
+  }
+  *out = p;
+  return CRT_OK;
+}
+
+int plan_set_nq(void* hp, int64_t nq, cudaStream_t stream)
+{
+  Plan* p = (Plan*)hp;
+  if (nq < 0 || nq > p->max_nq) return fail(CRT_ERR_INVALID_ARG, "plan: nq out of range");
+  if (p->sort && nq != p->max_nq)
+    return fail(CRT_ERR_NOT_SUPPORTED, "plan: a window-sorting plan runs exactly max_nq windows");
+  set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, nq);
+  CRT_LAUNCHED(1);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CRT_OK : cuda_fail(e, "plan_set_nq");
+}
+
+int plan_launch(void* hp, cudaStream_t stream)
+{
+  Plan* p = (Plan*)hp;
+  const bool timed = p->ev[0] && profiling();
+  if (timed) cudaEventRecord(p->ev[2], stream);
+  cudaError_t e = cudaGraphLaunch(p->exec, stream);
+  CRT_LAUNCHED(p->sort ? 13 : 5);
+  if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
+  if (timed) {
+    // the captured event nodes are re-recorded by every replay: read them now
+    cudaEventRecord(p->ev[3], stream);
+    float k = 0.f, all = 0.f;
+    if (cudaEventSynchronize(p->ev[3]) == cudaSuccess &&
+        cudaEventElapsedTime(&k, p->ev[0], p->ev[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&all, p->ev[2], p->ev[3]) == cudaSuccess) {
+      prof_add("traverse_persistent", k);
+      prof_add("plan", all);
+    }
+  }
+  return CRT_OK;
+}
+
+int plan_destroy(void* hp)
+{
+  Plan* p = (Plan*)hp;
+  if (!p) return CRT_OK;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  for (auto ev : p->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->scratch) cudaFree(p->scratch);
+  delete p;
+  return CRT_OK;
+}
+
+}  // namespace crt

@@ -1,0 +1,236 @@
+/*
+ * crtree -- B200-native 2-D bounding-box R-tree: Z-order bulk load and
+ * batched window query behind a C ABI.
+ *
+ * The drop-in entry points replace the reference's (trxcllnt/curtree)
+ * header templates one for one; every declaration below names the reference
+ * interface it replaces (paths relative to that project's root).  The
+ * extended entry points add what the reference lacks: 64-bit result counts,
+ * caller-owned output with overflow-and-retry, explicit streams, persistent
+ * batches captured in CUDA graphs, and a serving loop.
+ *
+ * Conventions
+ *   - Every function returns a crt_status code; none exits, aborts or traps.
+ *     crt_last_error() gives a message for the calling thread's last failure.
+ *   - Pointers inside crt_bbox_f32 / crt_rtree_f32 / crt_idpair are device
+ *     pointers (cudaMalloc or equivalent), unless a function says otherwise.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).
+ *   - Arithmetic is the reference's: fp32 centre (xmin + xmax) / 2 truncated
+ *     to uint16 per axis, a 32-bit Morton key sorted as a signed int (stable),
+ *     fp32 min/max node boxes, and the closed-interval intersection test
+ *     !(q.xmin > b.xmax || q.xmax < b.xmin || q.ymin > b.ymax || q.ymax < b.ymin).
+ */
+#ifndef CRTREE_H_
+#define CRTREE_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* crt_stream_t; /* same type as cudaStream_t */
+
+typedef enum {
+  CRT_OK                  = 0,
+  CRT_ERR_INVALID_ARG     = 1, /* n < 1, fanout < 2, null pointer, n + R_sz > INT32_MAX ... */
+  CRT_ERR_OOM             = 2, /* a device or host allocation failed */
+  CRT_ERR_OVERFLOW_INT32  = 3, /* result count does not fit the reference's int sz */
+  CRT_ERR_OUTPUT_OVERFLOW = 4, /* caller-owned output too small; *required holds the size */
+  CRT_ERR_DEVICE_TIMEOUT  = 5, /* a bounded device-side wait ran out */
+  CRT_ERR_CUDA            = 6, /* a CUDA runtime call failed */
+  CRT_ERR_NOT_SUPPORTED   = 7,
+  CRT_ERR_BUSY            = 8  /* serving: admission rejected (queue or memory full) */
+} crt_status;
+
+/* Layout-identical to BBOX<float> (src/rtree.h:3-11). */
+typedef struct {
+  int sz;
+  float* xmin;
+  float* ymin;
+  float* xmax;
+  float* ymax;
+  int* id;
+} crt_bbox_f32;
+
+/* Layout-identical to RTREE<float> (src/rtree.h:13-23).  Nodes [0, sz): root
+ * first, then each level downward; the children of node i are
+ * [pos[i], pos[i] + len[i]); pos[i] >= sz means the children are boxes at
+ * sorted slots pos[i] - sz ... */
+typedef struct {
+  int sz;
+  int fanout;
+  float* xmin;
+  float* ymin;
+  float* xmax;
+  float* ymax;
+  int* pos;
+  int* len;
+} crt_rtree_f32;
+
+/* Layout-identical to IDPAIR (src/rtree.h:25-29): fid = box id, tid = query
+ * index. */
+typedef struct {
+  int sz;
+  int* fid;
+  int* tid;
+} crt_idpair;
+
+const char* crt_status_string(int status);
+const char* crt_last_error(void);
+/* Library version string and the number of kernels launched by this process
+ * so far (a cheap counter the benchmark reports). */
+const char* crt_version(void);
+uint64_t crt_kernel_launches(void);
+
+/* ---------------------------------------------------------------------- */
+/* Drop-in entry points                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces `template <class T> int build_rtree(BBOX<T>& d_box, RTREE<T>& d_rt)`
+ * (src/rtree_bulkload_thrust.cuh:62-213).
+ * Reads d_rt->fanout, sorts d_box IN PLACE into Z-order (its five arrays are
+ * permuted; id[] then holds the original ids), allocates the six node arrays
+ * of d_rt with cudaMalloc (free with crt_rtree_free or the reference's
+ * rt_d_free), fills them bit-exactly as the reference does, sets d_rt->sz and
+ * *out_r_sz to R_sz.  Returns after the tree is complete on the device.
+ * d_box->sz == 1 gives R_sz == 0, as in the reference; d_box->sz < 1 or
+ * fanout < 2 (where the reference never returns) give CRT_ERR_INVALID_ARG. */
+int crt_build_f32(crt_bbox_f32* d_box, crt_rtree_f32* d_rt, crt_stream_t stream,
+                  int32_t* out_r_sz);
+
+/* Replaces `bfs_frontier(const RTREE<T>&, const BBOX<T>& d_rbox,
+ * const BBOX<T>& d_qbox, IDPAIR& d_dq)` (src/rtree_bfs_frontier.cuh:292-529).
+ * d_rbox is the box set build sorted (same arrays as d_box after
+ * crt_build_f32).  Allocates d_dq->fid / d_dq->tid with cudaMalloc (free with
+ * crt_idpair_free or the reference's idpair_d_free) and fills them with every
+ * (box id, query index) pair whose boxes intersect, in unspecified order.
+ * Never overflows (the reference aborts when a 32-query block expands past
+ * 1024 nodes); results past INT32_MAX pairs give CRT_ERR_OVERFLOW_INT32.
+ * With R_sz == 0 (a one-box tree) the box is tested directly. */
+int crt_query_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                  const crt_bbox_f32* d_qbox, crt_idpair* d_dq, crt_stream_t stream);
+
+/* Replaces `bfs_thrust(...)` (src/rtree_bfs_thrust.cuh:59-256), which returns
+ * the same pair set as bfs_frontier; same contract as crt_query_f32. */
+int crt_query_thrust_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                         const crt_bbox_f32* d_qbox, crt_idpair* d_dq, crt_stream_t stream);
+
+/* Replace rt_d_free / idpair_d_free (src/utility.cuh:137-162, 187-195):
+ * cudaFree the arrays and null the pointers. */
+int crt_rtree_free(crt_rtree_f32* d_rt);
+int crt_idpair_free(crt_idpair* d_dq);
+
+/* ---------------------------------------------------------------------- */
+/* Extended entry points (no reference counterpart)                         */
+/* ---------------------------------------------------------------------- */
+
+/* Out-of-place build: reads d_in (unchanged), writes the Z-ordered boxes into
+ * the caller-allocated arrays of d_sorted (same sz), and writes the nodes into
+ * the caller-allocated arrays of d_rt (capacity crt_tree_size(sz, fanout)).
+ * Asynchronous on `stream`; scratch comes from the stream-ordered allocator. */
+int crt_build_into_f32(const crt_bbox_f32* d_in, crt_bbox_f32* d_sorted, crt_rtree_f32* d_rt,
+                       crt_stream_t stream);
+
+/* R_sz for n boxes at this fanout (exact integer ceiling per level), or -1. */
+int64_t crt_tree_size(int64_t n, int fanout);
+/* Number of levels (root .. leaf-parents) and the node count of each level,
+ * leaf-parent level first, as in the reference's levels vector. */
+int crt_tree_levels(int64_t n, int fanout, int64_t* levels, int max_levels);
+
+/* Query modes. */
+enum {
+  CRT_QUERY_PERSISTENT = 0, /* one persistent work-stealing launch, Morton-ordered windows */
+  CRT_QUERY_PLAIN      = 1  /* one warp per window in input order: count pass, scan, write pass */
+};
+
+typedef struct {
+  int mode;          /* CRT_QUERY_PERSISTENT or CRT_QUERY_PLAIN */
+  int sort_windows;  /* persistent: visit windows in Morton order of their centres (default 1) */
+  int stage_levels;  /* persistent: stage the top tree levels in shared memory (default 1) */
+  int warps_per_cta; /* 0 = default */
+  int chunk;         /* persistent: output slots a warp reserves at a time (0 = default) */
+  int reserved[3];
+} crt_query_opts;
+
+void crt_query_opts_default(crt_query_opts* o);
+
+/* Device-resident result block of an extended query (caller-allocated,
+ * 64 bytes, device memory).  count = pairs written (valid when overflow == 0),
+ * required = exact pair count, overflow = 1 when required > capacity,
+ * error = a crt_status raised on the device. */
+typedef struct {
+  int64_t count;
+  int64_t required;
+  int32_t overflow;
+  int32_t error;
+  int64_t reserved[5];
+} crt_query_result;
+
+/* Windows against a tree into caller-owned output.  Asynchronous: enqueues
+ * the work on `stream` and writes *d_result on the device.  When the output is
+ * too small, d_result->overflow is set and d_result->required holds the exact
+ * pair count: grow the output to crt_query_capacity(required, ...) and call
+ * again (overflow-and-retry).  PLAIN mode also writes per-window hit counts
+ * (int64, nq + 1 entries, exclusive prefix) into d_offsets when non-NULL, and
+ * its pairs come grouped by window in window order. */
+int crt_query_into_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                       const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
+                       int64_t capacity, crt_query_result* d_result, int64_t* d_offsets,
+                       const crt_query_opts* opts, crt_stream_t stream);
+
+/* Output slots to allocate for `pairs` hit pairs so that a PERSISTENT query
+ * cannot overflow (adds the per-warp reservation slack). */
+int64_t crt_query_capacity(int64_t pairs, const crt_query_opts* opts);
+
+/* Synchronous convenience over crt_query_into_f32: runs, reads the result
+ * block, and returns CRT_ERR_OUTPUT_OVERFLOW with *required set when the
+ * output was too small. */
+int crt_query_sync_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                       const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
+                       int64_t capacity, int64_t* count, int64_t* required,
+                       const crt_query_opts* opts, crt_stream_t stream);
+
+/* Per-window workload statistics: hit count and number of leaf boxes tested
+ * (int64 device arrays of nq entries, either may be NULL); totals[0] = all
+ * hits, totals[1] = all leaf boxes tested (host, may be NULL).  Synchronous.
+ * Sizes outputs before a query and gives the benchmark its algorithmic bytes. */
+int crt_query_stats_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                        const crt_bbox_f32* d_qbox, int64_t* d_hits, int64_t* d_tested,
+                        int64_t* totals, crt_stream_t stream);
+
+/* Persistent batch plan: binds a tree, a window buffer of up to max_nq
+ * windows and an output buffer, and records the whole query (counter reset,
+ * window ordering, persistent traversal, output compaction) as one CUDA
+ * graph.  crt_plan_launch replays it for the windows currently in the bound
+ * buffer (nq may change between launches; the graph reads it from device
+ * memory).  The plan owns its scratch. */
+typedef struct crt_plan_s* crt_plan;
+int crt_plan_create(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                    const crt_bbox_f32* d_qbox, int64_t max_nq, int32_t* d_fid, int32_t* d_tid,
+                    int64_t capacity, crt_query_result* d_result, const crt_query_opts* opts,
+                    crt_stream_t stream, crt_plan* out);
+int crt_plan_set_nq(crt_plan plan, int64_t nq, crt_stream_t stream);
+int crt_plan_launch(crt_plan plan, crt_stream_t stream);
+int crt_plan_destroy(crt_plan plan);
+
+/* ---------------------------------------------------------------------- */
+/* Kernel timing (no reference counterpart; the reference prints host        */
+/* gettimeofday timers, src/rtree_bulkload_thrust.cuh:74-89)                */
+/* ---------------------------------------------------------------------- */
+
+/* When enabled, the library brackets each major kernel launch (encode,
+ * onesweep passes, level reductions, query traversal kernels, graph replays)
+ * with CUDA events on its own stream.  crt_profile_collect waits for them and
+ * sums the durations of the launches named `name` (all when NULL/empty):
+ * "encode", "sort_pass", "level", "traverse_persistent", "traverse_plain",
+ * "plan". */
+void crt_profile_enable(int on);
+int crt_profile_collect(const char* name, double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRTREE_H_ */

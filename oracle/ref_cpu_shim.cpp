@@ -1,0 +1,86 @@
+// C entry points around the reference's own CPU brute force
+// (nested_loop_query, src/utility.h:22-45), compiled from the reference
+// sources where they lie into oracle/_ref/libref_cpu.so by oracle/Makefile.
+// TEST INFRASTRUCTURE ONLY: used to pin the oracle and as the timed CPU
+// baseline of the benchmark; never linked into the product library.
+#include <cassert>
+#include <cstdint>
+#include <cstdio>
+#include <iostream>
+#include <iterator>
+#include <thread>
+#include <vector>
+
+#include <thrust/copy.h>
+#include <thrust/equal.h>
+#include <thrust/execution_policy.h>
+#include <thrust/host_vector.h>
+#include <thrust/iterator/constant_iterator.h>
+#include <thrust/reduce.h>
+
+#include "rtree.h"
+#include "utility.h"
+
+namespace {
+BBOX<float> make_box(const float* xmin, const float* ymin, const float* xmax, const float* ymax,
+                     const int* id, int n)
+{
+  BBOX<float> b;
+  b.sz   = n;
+  b.xmin = const_cast<float*>(xmin);
+  b.ymin = const_cast<float*>(ymin);
+  b.xmax = const_cast<float*>(xmax);
+  b.ymax = const_cast<float*>(ymax);
+  b.id   = const_cast<int*>(id);
+  return b;
+}
+}  // namespace
+
+// Runs the reference nested_loop_query once and copies up to `cap` pairs
+// (did, qid) out in the reference's order.  Returns the pair count.
+extern "C" int64_t ref_nested_loop_query(const float* qxmin, const float* qymin,
+                                         const float* qxmax, const float* qymax, const int* qid,
+                                         int nq, const float* dxmin, const float* dymin,
+                                         const float* dxmax, const float* dymax, const int* did,
+                                         int nd, int* out_did, int* out_qid, int64_t cap)
+{
+  BBOX<float> q = make_box(qxmin, qymin, qxmax, qymax, qid, nq);
+  BBOX<float> d = make_box(dxmin, dymin, dxmax, dymax, did, nd);
+  thrust::host_vector<int> v_did, v_qid;
+  int n = nested_loop_query<float>(q, d, v_did, v_qid);
+  for (int64_t i = 0; i < n && i < cap; i++) {
+    out_did[i] = v_did[i];
+    out_qid[i] = v_qid[i];
+  }
+  return n;
+}
+
+// Runs nested_loop_query over `nthreads` contiguous query slices, one host
+// thread each; returns the total pair count.  This is the multi-core form of
+// the reference's CPU path timed by the benchmark's reference arm.
+extern "C" int64_t ref_nested_loop_query_mt(const float* qxmin, const float* qymin,
+                                            const float* qxmax, const float* qymax,
+                                            const int* qid, int nq, const float* dxmin,
+                                            const float* dymin, const float* dxmax,
+                                            const float* dymax, const int* did, int nd,
+                                            int nthreads)
+{
+  if (nthreads < 1) nthreads = 1;
+  std::vector<int64_t> counts(nthreads, 0);
+  std::vector<std::thread> th;
+  int per = (nq + nthreads - 1) / nthreads;
+  for (int t = 0; t < nthreads; t++) {
+    int q0 = t * per, q1 = std::min(nq, (t + 1) * per);
+    if (q0 >= q1) break;
+    th.emplace_back([=, &counts] {
+      BBOX<float> q = make_box(qxmin + q0, qymin + q0, qxmax + q0, qymax + q0, qid + q0, q1 - q0);
+      BBOX<float> d = make_box(dxmin, dymin, dxmax, dymax, did, nd);
+      thrust::host_vector<int> v_did, v_qid;
+      counts[t] = nested_loop_query<float>(q, d, v_did, v_qid);
+    });
+  }
+  for (auto& t : th) t.join();
+  int64_t total = 0;
+  for (auto c : counts) total += c;
+  return total;
+}

@@ -1,0 +1,239 @@
+"""Window-query parity on the GPU: every form (drop-in bfs_frontier /
+bfs_thrust, plain, persistent, graph plan) returns exactly the oracle's hit
+pairs, through the C ABI, on the reference's edge cases."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from curtree_b200 import datasets as D
+from curtree_b200.datasets import HostBoxes
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def crt():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import curtree_b200 as C
+    C._lib.load()
+    return C
+
+
+def canon(fid, tid):
+    fid = fid.cpu().numpy() if hasattr(fid, "cpu") else np.asarray(fid)
+    tid = tid.cpu().numpy() if hasattr(tid, "cpu") else np.asarray(tid)
+    return O.canonical_pairs(fid, tid)
+
+
+def setup(crt, b, q, f=10):
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(f)
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    sb, t = O.build(b, f)
+    want = O.canonical_pairs(*O.tree_query_pairs(t, sb, q))
+    return d, rt, dq, want
+
+
+def all_forms(crt, d, rt, dq):
+    out = {}
+    p = crt.bfs_frontier(rt, d, dq)
+    out["frontier"] = canon(*p.to_host())
+    p.free()
+    p = crt.bfs_thrust(rt, d, dq)
+    out["thrust"] = canon(*p.to_host())
+    p.free()
+    out["plain"] = canon(*crt.query(rt, d, dq, mode=crt.CRT_QUERY_PLAIN)[:2])
+    out["persistent"] = canon(*crt.query(rt, d, dq))
+    out["persistent_unsorted"] = canon(*crt.query(rt, d, dq, sort_windows=0))
+    out["persistent_unstaged"] = canon(*crt.query(rt, d, dq, stage_levels=0))
+    out["persistent_small_chunk"] = canon(*crt.query(rt, d, dq, chunk=64))
+    return out
+
+
+def assert_all(out, want):
+    for k, v in out.items():
+        assert np.array_equal(v[0], want[0]) and np.array_equal(v[1], want[1]), k
+
+
+@pytest.mark.parametrize("f", [2, 3, 8, 10, 16, 32, 40])
+def test_query_fanouts(crt, f):
+    b = D.uniform_boxes(60_000, seed=40 + f)
+    q = D.mixed_windows(2000, b, seed=140 + f, lo=1e-4, hi=5e-2)
+    d, rt, dq, want = setup(crt, b, q, f)
+    assert len(want[0]) > 0
+    assert_all(all_forms(crt, d, rt, dq), want)
+
+
+def test_query_uniform_1m_10k_matches_brute_force(crt):
+    """1M boxes, 10k windows, fanout 10: pairs equal the brute force's."""
+    b = D.uniform_boxes(1_000_000, seed=1)
+    q = D.uniform_windows(10_000, seed=101)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    got = canon(*crt.query(rt, d, dq))
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    c, h = O.nested_loop_stats(q, b)
+    gc, gh = O.pair_hashes(got[0], got[1], q.n)
+    assert np.array_equal(gc, c) and np.array_equal(gh, h)
+    p = crt.bfs_frontier(rt, d, dq)
+    g2 = canon(*p.to_host())
+    assert np.array_equal(g2[0], want[0]) and np.array_equal(g2[1], want[1])
+
+
+def test_query_touching_edges_points_and_duplicates(crt):
+    b = D.uniform_boxes(20_000, seed=50)
+    b.xmax[::9] = b.xmin[::9]  # zero-width
+    b.ymax[::9] = b.ymin[::9]
+    for a in (b.xmin, b.ymin, b.xmax, b.ymax):
+        a[500:700] = a[499]  # duplicates
+    q = b.take(np.arange(0, 20_000, 37))  # windows equal to boxes: touching edges
+    q.id = np.arange(q.n, dtype=np.int32)
+    pts = D.uniform_windows(300, seed=150, max_side=0.0)  # point windows
+    q = HostBoxes.concat([q, pts])
+    q.id = np.arange(q.n, dtype=np.int32)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    assert_all(all_forms(crt, d, rt, dq), want)
+
+
+def test_query_all_miss_and_empty_batches(crt):
+    b = D.uniform_boxes(10_000, seed=51)
+    far = HostBoxes(*(np.full(100, v, np.float32) for v in (1e6, 1e6, 1e6 + 1, 1e6 + 1)),
+                    np.arange(100, dtype=np.int32))
+    d, rt, dq, want = setup(crt, b, far, 10)
+    assert len(want[0]) == 0
+    assert_all(all_forms(crt, d, rt, dq), want)
+    empty = HostBoxes(*(np.zeros(0, np.float32) for _ in range(4)), np.zeros(0, np.int32))
+    de = crt.BBox.from_host(empty)
+    fid, tid = crt.query(rt, d, de)
+    assert fid.numel() == 0
+    fid, tid, offs = crt.query(rt, d, de, mode=crt.CRT_QUERY_PLAIN)
+    assert fid.numel() == 0
+
+
+def test_query_one_box_tree(crt):
+    b = D.uniform_boxes(1, seed=52)
+    q = HostBoxes.concat([b, D.uniform_windows(50, seed=152, max_side=0.5)])
+    q.id = np.arange(q.n, dtype=np.int32)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(10)
+    assert crt.build_rtree(d, rt) == 0
+    dq = crt.BBox.from_host(q)
+    want = O.canonical_pairs(*O.nested_loop_pairs(q, b))
+    assert len(want[0]) >= 1
+    assert_all(all_forms(crt, d, rt, dq), want)
+
+
+def test_query_nan_window_follows_tree_semantics(crt):
+    """A NaN coordinate never excludes (src/rtree_bfs_frontier.cuh:40-44), so a
+    NaN window descends everywhere and hits every box."""
+    b = D.uniform_boxes(5_000, seed=53)
+    q = D.uniform_windows(20, seed=153)
+    q.xmin[3] = np.nan
+    d, rt, dq, want = setup(crt, b, q, 10)
+    assert (want[1] == 3).sum() == b.n
+    assert_all(all_forms(crt, d, rt, dq), want)
+
+
+def test_overflow_and_retry(crt):
+    import torch
+    b = D.uniform_boxes(100_000, seed=54)
+    q = D.uniform_windows(3000, seed=154, max_side=0.05)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    total = len(want[0])
+    for mode in (crt.CRT_QUERY_PERSISTENT, crt.CRT_QUERY_PLAIN):
+        res = crt.new_result_block()
+        cap = 1000
+        fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+        tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+        offs = torch.empty(q.n + 1, dtype=torch.int64, device="cuda") if mode else None
+        crt.query_into(rt, d, dq, fid, tid, res, offs, mode)
+        r = crt.read_result(res)
+        assert r["overflow"] == 1 and r["required"] == total
+        cap = crt.query_capacity(r["required"], mode)
+        fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+        tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+        crt.query_into(rt, d, dq, fid, tid, res, offs, mode)
+        r = crt.read_result(res)
+        assert r["overflow"] == 0 and r["count"] == total
+        got = canon(fid[:total], tid[:total])
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_plain_offsets_are_csr(crt):
+    b = D.uniform_boxes(50_000, seed=55)
+    q = D.uniform_windows(1000, seed=155)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    fid, tid, offs = crt.query(rt, d, dq, mode=crt.CRT_QUERY_PLAIN)
+    offs = offs.cpu().numpy()
+    tid = tid.cpu().numpy()
+    counts = np.bincount(want[1], minlength=q.n)
+    assert np.array_equal(np.diff(offs), counts)
+    # grouped by window in window order
+    assert np.all(np.diff(tid) >= 0)
+
+
+def test_plan_graph_replay(crt):
+    import torch
+    b = D.uniform_boxes(200_000, seed=56)
+    q = D.mixed_windows(5000, b, seed=156, lo=1e-4, hi=3e-2)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    cap = crt.query_capacity(len(want[0]))
+    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    res = crt.new_result_block()
+    plan = crt.Plan(rt, d, dq, fid, tid, res)
+    for _ in range(3):
+        fid.fill_(-1)
+        plan.launch()
+        r = crt.read_result(res)
+        assert r["overflow"] == 0 and r["count"] == len(want[0])
+        got = canon(fid[:r["count"]], tid[:r["count"]])
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    plan.destroy()
+    # an unsorted plan takes a smaller live window count
+    plan = crt.Plan(rt, d, dq, fid, tid, res, sort_windows=0)
+    plan.set_nq(1234)
+    plan.launch()
+    r = crt.read_result(res)
+    sel = want[1] < 1234
+    got = canon(fid[:r["count"]], tid[:r["count"]])
+    assert np.array_equal(got[0], want[0][sel]) and np.array_equal(got[1], want[1][sel])
+    plan.destroy()
+
+
+def test_mixed_windows_clustered_tree_counts(crt):
+    """Reduced instance of the uneven-window workload (log-uniform sides up to
+    0.1): per-window counts and pair digests equal the oracle's."""
+    b = D.clustered_boxes(2_000_000, seed=2, chunk=1_000_000)
+    q = D.mixed_windows(20_000, b, seed=157)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(16)
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    sb, t = O.build(b, 16)
+    st = O.tree_query_stats(t, sb, q)
+    fid, tid = crt.query(rt, d, dq)
+    assert fid.numel() == st.total
+    gc, gh = O.pair_hashes(fid.cpu().numpy(), tid.cpu().numpy(), q.n)
+    assert np.array_equal(gc, st.counts) and np.array_equal(gh, st.hashes)
+
+
+GOLDEN = [p for p in sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+          if "frontier_fid" in np.load(p)]
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_query_matches_reference_golden(crt, path):
+    z = np.load(path)
+    b = HostBoxes(z["box_xmin"], z["box_ymin"], z["box_xmax"], z["box_ymax"], z["box_id"])
+    q = HostBoxes(z["win_xmin"], z["win_ymin"], z["win_xmax"], z["win_ymax"], z["win_id"])
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(int(z["fanout"]))
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    want = (z["frontier_fid"], z["frontier_tid"])
+    assert_all(all_forms(crt, d, rt, dq), want)
