@@ -242,7 +242,7 @@ def run_ours(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
     step_ms = ms_max / args.steps
-    kern_ms = k_ms / max(k_n, 1)
+    kern_ms = k_ms / max(k_n, 1) if k_n else step_ms
     alg_bytes = 16 * args.windows + 16 * tested + 12 * pairs
     out["persistent"] = {"ms_per_step": step_ms, "windows_per_s": world * args.windows / (step_ms / 1e3),
                          "kernel_ms": kern_ms}

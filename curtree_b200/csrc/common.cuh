@@ -69,13 +69,11 @@ __device__ __forceinline__ uint32_t dilate16(uint32_t x)
 }
 
 // The reference's `(ushort)` cast of an fp32 centre
-// (src/rtree_bulkload_thrust.cuh:55-56) as the device performs it: toward
-// zero, saturating to [0, 65535], NaN -> 0.
-__device__ __forceinline__ uint32_t f2u16(float v)
-{
-  uint32_t u = __float2uint_rz(v);
-  return u > 65535u ? 65535u : u;
-}
+// (src/rtree_bulkload_thrust.cuh:55-56) as its device build performs it:
+// truncate toward zero to an unsigned 32-bit integer (negative and NaN -> 0,
+// >= 2^32 -> 2^32 - 1), then keep the low 16 bits.  Pinned against the
+// reference's own build on centres outside [0, 65536).
+__device__ __forceinline__ uint32_t f2u16(float v) { return __float2uint_rz(v) & 0xFFFFu; }
 
 // mbr2key (src/rtree_bulkload_thrust.cuh:52-60) with bit 31 flipped, so that
 // the reference's signed-int key order (src/rtree_bulkload_thrust.cuh:72,

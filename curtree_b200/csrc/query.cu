@@ -772,26 +772,39 @@ static void persist_scratch_carve(char* base, int64_t max_nq, long long max_hole
   S.bytes = off;
 }
 
-// Enqueues one persistent query (no host synchronisation).  `nq_dev` is read
-// from S.ctr->nq, which the caller sets (set_nq_kernel) before.
-static void enqueue_persistent(const TreeView& T, const WindowView& W, int64_t max_nq,
-                               const PersistScratch& S, bool sort, int stage_n, int32_t* fid,
-                               int32_t* tid, long long cap, int chunk, crt_query_result* res,
-                               cudaStream_t stream, cudaEvent_t ev0 = nullptr,
-                               cudaEvent_t ev1 = nullptr)
+// A persistent query is three stages on one stream, none synchronising the
+// host: `pre` (reset the counters, order the windows), the traversal kernel,
+// and `post` (sort the unused chunk ends, compact, write the result block).
+// The plan records pre and post as CUDA graphs and launches the traversal
+// between them, so its duration can be taken with ordinary events.
+static void enqueue_pre(const WindowView& W, int64_t max_nq, const PersistScratch& S, bool sort,
+                        cudaStream_t stream)
 {
-  const TraversalShape sh = traversal_shape(T.nbox, T.fanout);
   // counters (keep nq) and the sort's zeroed block
   cudaMemsetAsync(S.ctr, 0, offsetof(QueryCounters, nq), stream);
-  const int sms = sm_count();
   if (sort && max_nq > 0) {
+    const int sms = sm_count();
     cudaMemsetAsync(S.sort_zero, 0, sort_zero_bytes(max_nq), stream);
     int g = (int)std::min<int64_t>(cdiv(max_nq, 256), (int64_t)sms * 4);
     window_key_kernel<<<std::max(g, 1), 256, 0, stream>>>(W, S.bufs.keys[0], sort_hist(S.sort_zero));
     sort_passes(S.bufs, W.n, S.sort_zero, stream);
     CRT_LAUNCHED(1);
   }
+}
+
+struct TraverseLaunch {
   PersistParams P;
+  size_t smem;
+  int grid;
+};
+
+static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
+                                    const PersistScratch& S, bool sort, int stage_n,
+                                    int32_t* fid, int32_t* tid, long long cap, int chunk)
+{
+  const TraversalShape sh = traversal_shape(T.nbox, T.fanout);
+  TraverseLaunch L;
+  PersistParams& P = L.P;
   P.T = T;
   P.W = W;
   P.order0 = S.bufs.vals[0];
@@ -807,21 +820,29 @@ static void enqueue_persistent(const TreeView& T, const WindowView& W, int64_t m
   P.ctr = S.ctr;
   P.holes = S.holes;
   P.max_holes = S.max_holes;
-  const size_t smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
-  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int grid = persistent_grid(smem);
-  {
-    ProfScope ps("traverse_persistent", stream);
-    if (ev0) cudaEventRecord(ev0, stream);
-    persistent_kernel<<<grid, kPersistThreads, smem, stream>>>(P);
-    if (ev1) cudaEventRecord(ev1, stream);
-  }
+  L.smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
+  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
+  L.grid = persistent_grid(L.smem);
+  return L;
+}
+
+static void launch_traverse(const TraverseLaunch& L, cudaStream_t stream)
+{
+  ProfScope ps("traverse_persistent", stream);
+  persistent_kernel<<<L.grid, kPersistThreads, L.smem, stream>>>(L.P);
+  CRT_LAUNCHED(1);
+}
+
+static void enqueue_post(const PersistScratch& S, int32_t* fid, int32_t* tid, long long cap,
+                         crt_query_result* res, cudaStream_t stream)
+{
+  const int sms = sm_count();
   hole_sort_kernel<<<std::max(1, (int)cdiv(S.max_holes, 256)), 256, 0, stream>>>(
       S.holes, S.sorted, S.ctr, S.max_holes);
   hole_prefix_kernel<<<1, kScanThreads, 0, stream>>>(S.sorted, S.cum, S.ctr, S.max_holes);
   compact_kernel<<<sms * 4, 256, 0, stream>>>(S.sorted, S.cum, S.ctr, S.max_holes, fid, tid,
                                               cap, res);
-  CRT_LAUNCHED(4);
+  CRT_LAUNCHED(3);
 }
 
 static int stage_nodes_for(const crt_rtree_f32& rt, bool want)
@@ -917,7 +938,9 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   persist_scratch_carve(scr, nq, max_holes, sort, S);
   set_nq_kernel<<<1, 1, 0, stream>>>(S.ctr, nq);
   CRT_LAUNCHED(1);
-  enqueue_persistent(T, W, nq, S, sort, stage_n, fid, tid, capacity, chunk, d_result, stream);
+  enqueue_pre(W, nq, S, sort, stream);
+  launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk), stream);
+  enqueue_post(S, fid, tid, capacity, d_result, stream);
   cudaFreeAsync(scr, stream);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "query (persistent)");
@@ -977,10 +1000,12 @@ struct Plan {
   int32_t* tid;
   long long cap;
   crt_query_result* res;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // kernel pair, replay pair
+  TraverseLaunch traverse;
+  cudaGraph_t graph[2] = {nullptr, nullptr};  // pre, post
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
 };
+
+int plan_destroy(void* hp);
 
 int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
                 int64_t max_nq, int32_t* fid, int32_t* tid, int64_t capacity,
@@ -1012,31 +1037,32 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   persist_scratch_carve(p->scratch, max_nq, max_holes, p->sort, p->S);
   cudaMemsetAsync(p->S.ctr, 0, sizeof(QueryCounters), stream);
   set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
-  // capture on a private stream
+  p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk);
+  // capture pre and post on a private stream
   cudaStream_t cs;
   if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFree(p->scratch);
     delete p;
     return cuda_fail(cudaGetLastError(), "plan: stream");
   }
-  if (profiling())
-    for (auto& ev : p->ev) cudaEventCreate(&ev);
-  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    // a window-sorting plan orders exactly max_nq windows, so it only runs
-    // with nq == max_nq (plan_set_nq enforces it); without sorting the
-    // kernel reads the live count from ctr->nq
-    enqueue_persistent(p->T, p->W, max_nq, p->S, p->sort, p->stage_n, fid, tid, capacity,
-                       p->chunk, res, cs, p->ev[0], p->ev[1]);
-    e = cudaStreamEndCapture(cs, &p->graph);
+  // a window-sorting plan orders exactly max_nq windows, so it only runs with
+  // nq == max_nq (plan_set_nq enforces it); without sorting the kernel reads
+  // the live count from ctr->nq
+  cudaError_t e = cudaSuccess;
+  for (int g = 0; g < 2 && e == cudaSuccess; g++) {
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) break;
+    if (g == 0)
+      enqueue_pre(p->W, max_nq, p->S, p->sort, cs);
+    else
+      enqueue_post(p->S, fid, tid, capacity, res, cs);
+    e = cudaStreamEndCapture(cs, &p->graph[g]);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec[g], p->graph[g], 0);
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
   cudaStreamSynchronize(stream);
   cudaStreamDestroy(cs);
   if (e != cudaSuccess) {
-    if (p->graph) cudaGraphDestroy(p->graph);
-    cudaFree(p->scratch);
-    delete p;
+    plan_destroy(p);
     return cuda_fail(e, "plan: graph capture");
   }
   *out = p;
@@ -1058,22 +1084,13 @@ int plan_set_nq(void* hp, int64_t nq, cudaStream_t stream)
 int plan_launch(void* hp, cudaStream_t stream)
 {
   Plan* p = (Plan*)hp;
-  const bool timed = p->ev[0] && profiling();
-  if (timed) cudaEventRecord(p->ev[2], stream);
-  cudaError_t e = cudaGraphLaunch(p->exec, stream);
-  CRT_LAUNCHED(p->sort ? 13 : 5);
+  cudaError_t e = cudaGraphLaunch(p->exec[0], stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
-  if (timed) {
-    // the captured event nodes are re-recorded by every replay: read them now
-    cudaEventRecord(p->ev[3], stream);
-    float k = 0.f, all = 0.f;
-    if (cudaEventSynchronize(p->ev[3]) == cudaSuccess &&
-        cudaEventElapsedTime(&k, p->ev[0], p->ev[1]) == cudaSuccess &&
-        cudaEventElapsedTime(&all, p->ev[2], p->ev[3]) == cudaSuccess) {
-      prof_add("traverse_persistent", k);
-      prof_add("plan", all);
-    }
-  }
+  CRT_LAUNCHED(p->sort ? 7 : 0);
+  launch_traverse(p->traverse, stream);
+  e = cudaGraphLaunch(p->exec[1], stream);
+  CRT_LAUNCHED(3);
+  if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
   return CRT_OK;
 }
 
@@ -1081,10 +1098,10 @@ int plan_destroy(void* hp)
 {
   Plan* p = (Plan*)hp;
   if (!p) return CRT_OK;
-  if (p->exec) cudaGraphExecDestroy(p->exec);
-  for (auto ev : p->ev)
-    if (ev) cudaEventDestroy(ev);
-  if (p->graph) cudaGraphDestroy(p->graph);
+  for (int g = 0; g < 2; g++) {
+    if (p->exec[g]) cudaGraphExecDestroy(p->exec[g]);
+    if (p->graph[g]) cudaGraphDestroy(p->graph[g]);
+  }
   if (p->scratch) cudaFree(p->scratch);
   delete p;
   return CRT_OK;

@@ -31,15 +31,17 @@
 /* Morton key                                                                */
 /* ------------------------------------------------------------------------ */
 
-/* Float -> uint16 conversion as the device performs it for the reference's
- * `(ushort)` cast (src/rtree_bulkload_thrust.cuh:55-56): round toward zero,
- * saturate to [0, 65535], NaN -> 0. */
+/* Float -> uint16 conversion as the reference's device build performs its
+ * `(ushort)` cast (src/rtree_bulkload_thrust.cuh:55-56): truncate toward zero
+ * to an unsigned 32-bit integer, saturating (negative and NaN -> 0,
+ * >= 2^32 -> 2^32 - 1), then keep the low 16 bits.  Pinned by the golden
+ * fixtures whose box centres lie outside [0, 65536). */
 uint16_t orc_f2u16(float v)
 {
   if (v != v) return 0;
   if (v <= 0.0f) return 0;
-  if (v >= 65535.0f) return 65535;
-  return (uint16_t)v;
+  if (v >= 4294967296.0f) return 0xFFFF;
+  return (uint16_t)((uint32_t)v & 0xFFFFu);
 }
 
 /* Spread the 16 bits of v over the even bit positions of a 32-bit word: the

@@ -128,13 +128,17 @@ def test_query_one_box_tree(crt):
 
 
 def test_query_nan_window_follows_tree_semantics(crt):
-    """A NaN coordinate never excludes (src/rtree_bfs_frontier.cuh:40-44), so a
-    NaN window descends everywhere and hits every box."""
+    """A NaN coordinate never excludes (src/rtree_bfs_frontier.cuh:40-44): an
+    all-NaN window descends everywhere and hits every box; a window with one
+    NaN side is bounded by the other three."""
     b = D.uniform_boxes(5_000, seed=53)
     q = D.uniform_windows(20, seed=153)
-    q.xmin[3] = np.nan
+    for a in (q.xmin, q.ymin, q.xmax, q.ymax):
+        a[3] = np.nan
+    q.xmin[7] = np.nan
     d, rt, dq, want = setup(crt, b, q, 10)
     assert (want[1] == 3).sum() == b.n
+    assert 0 < (want[1] == 7).sum() < b.n
     assert_all(all_forms(crt, d, rt, dq), want)
 
 

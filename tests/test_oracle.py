@@ -46,10 +46,13 @@ def test_key_examples():
     assert O.lib().orc_key(0.0, 0.0, 3.9, 0.0) == O.lib().orc_key(1.0, 0.0, 1.0, 0.0)
     # y >= 2^15 sets bit 31: a negative signed key
     assert O.lib().orc_key(0.0, 40000.0, 0.0, 40000.0) < 0
-    # saturation and NaN, as the device converts
-    assert O.lib().orc_f2u16(70000.0) == 65535
+    # out-of-range centres, as the reference's device build converts them:
+    # unsigned 32-bit truncation (saturating), then the low 16 bits
+    assert O.lib().orc_f2u16(70000.0) == 70000 & 0xFFFF
+    assert O.lib().orc_f2u16(65536.0) == 0
     assert O.lib().orc_f2u16(-5.0) == 0
     assert O.lib().orc_f2u16(float("nan")) == 0
+    assert O.lib().orc_f2u16(1e12) == 0xFFFF
 
 
 def test_sort_is_stable_and_signed():
