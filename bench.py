@@ -58,7 +58,15 @@ def parse():
     p.add_argument("--build-boxes", type=int, default=BUILD_BOXES)
     p.add_argument("--fanout", type=int, default=FANOUT)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
-    p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu")
+    p.add_argument("--warps", type=int, default=0, help="warps per CTA of the persistent traversal")
+    p.add_argument("--stage", type=int, default=1, help="stage the top tree levels in shared memory")
+    p.add_argument("--sort-windows", type=int, default=1)
+    p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu,serve")
+    p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
+    p.add_argument("--serve-requests", type=int, default=300)
+    p.add_argument("--serve-rate", type=float, default=500.0)
+    p.add_argument("--serve-max-batch", type=int, default=100_000)
+    p.add_argument("--serve-arena-gb", type=int, default=64)
     return p.parse_args()
 
 
@@ -219,7 +227,9 @@ def run_ours(args, rank, world, dist):
 
     # ---- persistent form (graph plan) -------------------------------------
     L.crt_profile_enable(1)
-    plan = C.Plan(rt, sorted_box, d_win, fid, tid, res)
+    qopts = {"warps_per_cta": args.warps, "stage_levels": args.stage,
+             "sort_windows": args.sort_windows}
+    plan = C.Plan(rt, sorted_box, d_win, fid, tid, res, **qopts)
     for _ in range(args.warmup):
         plan.launch()
     torch.cuda.synchronize()
@@ -245,7 +255,7 @@ def run_ours(args, rank, world, dist):
     kern_ms = k_ms / max(k_n, 1) if k_n else step_ms
     alg_bytes = 16 * args.windows + 16 * tested + 12 * pairs
     out["persistent"] = {"ms_per_step": step_ms, "windows_per_s": world * args.windows / (step_ms / 1e3),
-                         "kernel_ms": kern_ms}
+                         "kernel_ms": kern_ms, "opts": qopts}
     out["roofline"] = {"bound": "hbm", "achieved": alg_bytes / (kern_ms / 1e3) / 1e9,
                        "peak": hbm_peak, "unit": "GB/s",
                        "frac": alg_bytes / (kern_ms / 1e3) / 1e9 / hbm_peak,
@@ -290,6 +300,11 @@ def run_ours(args, rank, world, dist):
     L.crt_profile_enable(0)
     del fid, tid
     torch.cuda.empty_cache()
+
+    # ---- serving loop -----------------------------------------------------------
+    if "serve" not in skip:
+        out["serving"] = serving_leg(args, C, rank)
+        torch.cuda.empty_cache()
 
     # ---- bulk load ------------------------------------------------------------
     if "build" not in skip:
@@ -338,6 +353,123 @@ def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, d
     return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * pairs + 64,
             "ms_per_step": ms / args.steps, "path": "crt_query_into_f32 (persistent) via ctypes"}
+
+
+def serving_workload(args, rank):
+    """Four device-resident trees (1M, 5M, 20M, 50M uniform boxes) and a
+    Poisson stream of requests: tree uniform, batch size log-uniform in
+    [1, 100k] windows, window side log-uniform in [1e-5, 1e-1]."""
+    from curtree_b200 import datasets as D
+    sizes = [int(x) for x in args.serve_trees.split(",")]
+    trees = [D.uniform_boxes(n, seed=41 + i) for i, n in enumerate(sizes)]
+    tree_idx, nq = D.serving_requests(args.serve_requests, len(trees), seed=104 + 1000 * rank,
+                                      hi=args.serve_max_batch)
+    rng = np.random.default_rng(204 + rank)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, args.serve_requests))
+    reqs = []
+    for i in range(args.serve_requests):
+        w = D.mixed_windows(int(nq[i]), trees[tree_idx[i]], seed=10_000 + 7 * i + 1000 * rank)
+        reqs.append((int(tree_idx[i]), w))
+    return trees, reqs, arrivals
+
+
+def serving_leg(args, C, rank):
+    import time
+
+    import torch
+
+    from curtree_b200.server import Server
+    trees, reqs, arrivals = serving_workload(args, rank)
+    built = []
+    for b in trees:
+        d = C.BBox.from_host(b)
+        rt = C.RTree(args.fanout)
+        C.build_rtree(d, rt)
+        built.append((rt, d))
+    total_windows = sum(w.n for _, w in reqs)
+
+    # ---- served: continuous batching ------------------------------------------
+    srv = Server(arena_bytes=args.serve_arena_gb << 30, pairs_per_window=256.0)
+    tids = [srv.add_tree(rt, d) for rt, d in built]
+    # warm the device loop and the per-tree output estimates
+    for i in range(min(8, len(reqs))):
+        while srv.submit(tids[reqs[i][0]], reqs[i][1]) is None:
+            time.sleep(1e-3)
+    got = 0
+    while got < min(8, len(reqs)):
+        for c in srv.poll(wait_ms=50):
+            srv.release(c["request_id"])
+            got += 1
+    lat = np.zeros(len(reqs))
+    pairs = 0
+    backlog = []
+    ids = {}
+    nxt = 0
+    done = 0
+    retries = 0
+    t0 = time.monotonic()
+    while done < len(reqs):
+        now = time.monotonic() - t0
+        while nxt < len(reqs) and arrivals[nxt] <= now:
+            backlog.append(nxt)
+            nxt += 1
+        while backlog:
+            i = backlog[0]
+            rid = srv.submit(tids[reqs[i][0]], reqs[i][1])
+            if rid is None:
+                break
+            ids[rid] = i
+            backlog.pop(0)
+        for c in srv.poll(max_out=256, wait_ms=0 if (backlog or nxt < len(reqs)) else 2):
+            i = ids.pop(c["request_id"])
+            if c["status"] != 0:
+                raise RuntimeError(f"served request failed: {c}")
+            lat[i] = c["complete_time_s"] - (t0 + arrivals[i])
+            pairs += c["count"]
+            retries += c["retries"]
+            srv.release(c["request_id"])
+            done += 1
+        if nxt < len(reqs) and not backlog:
+            time.sleep(max(0.0, min(2e-4, arrivals[nxt] - (time.monotonic() - t0))))
+    makespan = time.monotonic() - t0
+    srv.close()
+    served = {"windows_per_s": total_windows / makespan, "requests_per_s": len(reqs) / makespan,
+              "p50_ms": float(np.percentile(lat, 50) * 1e3),
+              "p99_ms": float(np.percentile(lat, 99) * 1e3), "makespan_s": makespan,
+              "pairs": int(pairs), "retries": int(retries)}
+
+    # ---- plain: one request at a time, plain per-batch form ----------------------
+    stats = []
+    for ti, w in reqs:
+        dq = C.BBox.from_host(w)
+        stats.append(C.query_stats(built[ti][0], built[ti][1], dq)["hits"])
+    cap = max(max(stats), 1)
+    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    res = C.new_result_block()
+    h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+    lat_p = np.zeros(len(reqs))
+    t0 = time.monotonic()
+    for i, (ti, w) in enumerate(reqs):
+        wait = arrivals[i] - (time.monotonic() - t0)
+        if wait > 0:
+            time.sleep(wait)
+        dq = C.BBox.from_host(w)
+        C.query_into(built[ti][0], built[ti][1], dq, fid, tid, res, None, C.CRT_QUERY_PLAIN)
+        h_res.copy_(res)
+        r = C.read_result(h_res)
+        assert r["count"] == stats[i], (r, stats[i])
+        lat_p[i] = time.monotonic() - (t0 + arrivals[i])
+    makespan_p = time.monotonic() - t0
+    plain = {"windows_per_s": total_windows / makespan_p, "requests_per_s": len(reqs) / makespan_p,
+             "p50_ms": float(np.percentile(lat_p, 50) * 1e3),
+             "p99_ms": float(np.percentile(lat_p, 99) * 1e3), "makespan_s": makespan_p}
+    assert served["pairs"] == sum(stats), (served["pairs"], sum(stats))
+    return {"workload": f"trees {args.serve_trees} uniform boxes, fanout {args.fanout}; "
+                        f"{len(reqs)} requests, Poisson {args.serve_rate:g} req/s, batch "
+                        f"log-U[1, {args.serve_max_batch}] windows, side log-U[1e-5, 1e-1]",
+            "windows": int(total_windows), "served": served, "plain": plain,
+            "served_vs_plain_windows_per_s": served["windows_per_s"] / plain["windows_per_s"]}
 
 
 def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
@@ -446,6 +578,7 @@ def main():
                 "roofline": out["roofline"], "cpu_baseline": cpu, "e2e": out.get("e2e"),
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
                 "plain": out.get("plain"), "build": out.get("build"),
+                "serving": out.get("serving"),
                 "workload_stats": out["workload_stats"],
                 "persistent_kernel_ms": p["kernel_ms"]}
         if "plain" in out:

@@ -59,6 +59,21 @@ class crt_query_result(ctypes.Structure):
                 ("reserved", ctypes.c_int64 * 5)]
 
 
+class crt_server_opts(ctypes.Structure):
+    _fields_ = [("arena_bytes", ctypes.c_int64), ("max_requests", ctypes.c_int),
+                ("max_trees", ctypes.c_int), ("pairs_per_window", ctypes.c_double),
+                ("output_slack", ctypes.c_double), ("idle_ms", ctypes.c_int),
+                ("device_wait_us", ctypes.c_int64), ("reserved", ctypes.c_int * 4)]
+
+
+class crt_server_completion(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_int64), ("tree_id", ctypes.c_int), ("status", ctypes.c_int),
+                ("nq", ctypes.c_int64), ("count", ctypes.c_int64), ("d_fid", ctypes.c_void_p),
+                ("d_tid", ctypes.c_void_p), ("submit_time_s", ctypes.c_double),
+                ("complete_time_s", ctypes.c_double), ("retries", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
 assert ctypes.sizeof(crt_bbox_f32) == 48
 assert ctypes.sizeof(crt_rtree_f32) == 56
 assert ctypes.sizeof(crt_idpair) == 24
@@ -111,6 +126,18 @@ SIGNATURES = {
     "crt_plan_set_nq": (ctypes.c_int, [_vp, _i64, _vp]),
     "crt_plan_launch": (ctypes.c_int, [_vp, _vp]),
     "crt_plan_destroy": (ctypes.c_int, [_vp]),
+    "crt_server_opts_default": (None, [ctypes.POINTER(crt_server_opts)]),
+    "crt_server_create": (ctypes.c_int, [ctypes.POINTER(crt_server_opts), ctypes.POINTER(_vp)]),
+    "crt_server_add_tree": (ctypes.c_int, [_vp, ctypes.POINTER(crt_rtree_f32),
+                                           ctypes.POINTER(crt_bbox_f32), ctypes.POINTER(ctypes.c_int)]),
+    "crt_server_submit": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _i64,
+                                         ctypes.POINTER(_i64)]),
+    "crt_server_poll": (ctypes.c_int, [_vp, ctypes.POINTER(crt_server_completion), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "crt_server_release": (ctypes.c_int, [_vp, _i64]),
+    "crt_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+                                        ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "crt_server_destroy": (ctypes.c_int, [_vp]),
     "crt_profile_enable": (None, [ctypes.c_int]),
     "crt_profile_collect": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(_i64)]),

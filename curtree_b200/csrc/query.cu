@@ -34,33 +34,9 @@
 
 #include "internal.h"
 #include "profile.h"
+#include "traverse.cuh"
 
 namespace crt {
-
-struct TreeView {
-  const float* __restrict__ nxmin;
-  const float* __restrict__ nymin;
-  const float* __restrict__ nxmax;
-  const float* __restrict__ nymax;
-  const int* __restrict__ npos;
-  const int* __restrict__ nlen;
-  int rsz;
-  int fanout;
-  const float* __restrict__ bxmin;
-  const float* __restrict__ bymin;
-  const float* __restrict__ bxmax;
-  const float* __restrict__ bymax;
-  const int* __restrict__ bid;
-  int nbox;
-};
-
-struct WindowView {
-  const float* __restrict__ xmin;
-  const float* __restrict__ ymin;
-  const float* __restrict__ xmax;
-  const float* __restrict__ ymax;
-  int64_t n;
-};
 
 // Device-side counters of one query (int64 words; zeroed before a launch).
 struct QueryCounters {
@@ -77,36 +53,6 @@ struct Hole {
   long long start;
   long long len;
 };
-
-// Top tree levels staged in shared memory (node index < n), or none.
-struct NodeCache {
-  const float* xmin;
-  const float* ymin;
-  const float* xmax;
-  const float* ymax;
-  const int* pos;
-  const int* len;
-  int n;
-};
-
-__device__ __forceinline__ void load_node_box(const TreeView& T, const NodeCache& C, int i,
-                                              float& a, float& b, float& c, float& d)
-{
-  if (i < C.n) {
-    a = C.xmin[i]; b = C.ymin[i]; c = C.xmax[i]; d = C.ymax[i];
-  } else {
-    a = __ldg(T.nxmin + i); b = __ldg(T.nymin + i); c = __ldg(T.nxmax + i); d = __ldg(T.nymax + i);
-  }
-}
-__device__ __forceinline__ void load_node_link(const TreeView& T, const NodeCache& C, int i,
-                                               int& p, int& l)
-{
-  if (i < C.n) {
-    p = C.pos[i]; l = C.len[i];
-  } else {
-    p = __ldg(T.npos + i); l = __ldg(T.nlen + i);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Emitters: warp-collective; `hit` and `id` are per lane.
@@ -190,98 +136,6 @@ struct ChunkEmit {
 };
 
 // ---------------------------------------------------------------------------
-// Warp traversal of one window
-// ---------------------------------------------------------------------------
-template <class Emit>
-__device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, int K,
-                                         int lane_g, int lane_c, float x1, float y1, float x2,
-                                         float y2, int* stack, int stack_cap, Emit& emit,
-                                         int* err)
-{
-  const int lane = (int)lane_id();
-  const uint32_t lt = lanemask_lt();
-  const int f = T.fanout;
-  if (T.rsz == 0) {
-    // one-box (or empty) tree: no nodes, test the boxes directly
-    for (int base = 0; base < T.nbox; base += 32) {
-      int s = base + lane;
-      bool hit = s < T.nbox &&
-                 intersects(x1, y1, x2, y2, T.bxmin[s], T.bymin[s], T.bxmax[s], T.bymax[s]);
-      if constexpr (Emit::kCountsTests) emit.leaf_tests(min(32, T.nbox - base));
-      emit(hit, hit ? T.bid[s] : 0);
-    }
-    return;
-  }
-  if (lane == 0) stack[0] = 0;
-  int sp = 1;
-  __syncwarp();
-  while (sp > 0) {
-    const int k = min(sp, K);
-    sp -= k;
-    // popped entries stack[sp .. sp+k): lower index = shallower; lane g holds entry g
-    int my_pos = 0, my_len = 0;
-    if (lane < k) load_node_link(T, C, stack[sp + lane], my_pos, my_len);
-    __syncwarp();
-    const int span = f <= 32 ? 32 : f;  // children covered per node group
-    for (int base = 0; base < span; base += 32) {
-      int g, c;
-      if (f <= 32) { g = lane_g; c = lane_c; }
-      else { g = 0; c = base + lane; }
-      const int gs = min(g, k - 1);
-      const int pos = __shfl_sync(0xffffffffu, my_pos, gs);
-      const int len = __shfl_sync(0xffffffffu, my_len, gs);
-      const bool valid = g < k && c < len;
-      const int child = pos + c;
-      bool hit = false, push = false;
-      int hid = 0;
-      if (valid) {
-        if (pos >= T.rsz) {
-          const int s = child - T.rsz;
-          if (s < T.nbox) {
-            hit = intersects(x1, y1, x2, y2, __ldg(T.bxmin + s), __ldg(T.bymin + s),
-                             __ldg(T.bxmax + s), __ldg(T.bymax + s));
-            if (hit) hid = __ldg(T.bid + s);
-          }
-        } else if (child < T.rsz) {
-          float a, b, cc, d;
-          load_node_box(T, C, child, a, b, cc, d);
-          push = intersects(x1, y1, x2, y2, a, b, cc, d);
-        }
-      }
-      if constexpr (Emit::kCountsTests)
-        emit.leaf_tests(__popc(__ballot_sync(0xffffffffu, valid && pos >= T.rsz && child - T.rsz < T.nbox)));
-      const uint32_t pm = __ballot_sync(0xffffffffu, push);
-      if (pm) {
-        const int np = __popc(pm);
-        if (sp + np > stack_cap) {
-          // cannot happen with the host-sized stack; never write past it
-          raise_error(err, CRT_ERR_NOT_SUPPORTED);
-          return;
-        }
-        if (push) stack[sp + __popc(pm & lt)] = child;
-        sp += np;
-      }
-      emit(hit, hid);
-    }
-    __syncwarp();
-  }
-}
-
-// Lane -> (node group, child) for fanout <= 32.
-__device__ __forceinline__ void lane_map(int f, int K, int& g, int& c)
-{
-  const int lane = (int)lane_id();
-  if (f <= 32) {
-    g = lane / f;
-    c = lane - g * f;
-    if (g >= K) { g = 32; c = 0; }
-  } else {
-    g = 0;
-    c = lane;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Plain form: count pass / write pass, one warp per window in input order
 // ---------------------------------------------------------------------------
 constexpr int kPlainWarps = 8;
@@ -290,7 +144,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
     plain_count_kernel(TreeView T, WindowView W, int K, int stack_cap,
                        long long* __restrict__ counts, QueryCounters* ctr)
 {
-  extern __shared__ int s_stack[];
+  extern __shared__ FrontierEntry s_stack[];
   const int warp = threadIdx.x >> 5;
   const long long q = (long long)blockIdx.x * kPlainWarps + warp;
   if (q >= W.n) return;
@@ -308,7 +162,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
                        const long long* __restrict__ offsets, int32_t* fid, int32_t* tid,
                        long long cap, QueryCounters* ctr)
 {
-  extern __shared__ int s_stack[];
+  extern __shared__ FrontierEntry s_stack[];
   const int warp = threadIdx.x >> 5;
   const long long q = (long long)blockIdx.x * kPlainWarps + warp;
   if (q >= W.n) return;
@@ -326,7 +180,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
                  long long* __restrict__ tested, unsigned long long* __restrict__ totals,
                  QueryCounters* ctr)
 {
-  extern __shared__ int s_stack[];
+  extern __shared__ FrontierEntry s_stack[];
   const int warp = threadIdx.x >> 5;
   const long long q = (long long)blockIdx.x * kPlainWarps + warp;
   if (q >= W.n) return;
@@ -450,7 +304,19 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p)
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__global__ void __launch_bounds__(256)
+// One bulk async copy global -> shared (16-byte aligned, size a multiple of
+// 16), completing on the mbarrier at `bar`.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
     persistent_kernel(PersistParams P)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -465,7 +331,7 @@ __global__ void __launch_bounds__(256)
   float* c_ymax = c_xmax + P.stage_n;
   int* c_pos = (int*)(c_ymax + P.stage_n);
   int* c_len = c_pos + P.stage_n;
-  int* stacks = c_len + P.stage_n;
+  FrontierEntry* stacks = (FrontierEntry*)(c_len + P.stage_n);
   NodeCache C{c_xmin, c_ymin, c_xmax, c_ymax, c_pos, c_len, 0};
 
   if (P.stage_n > 0) {
@@ -482,14 +348,12 @@ __global__ void __launch_bounds__(256)
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                    "r"(6u * bytes)
                    : "memory");
-      const void* src[6] = {P.T.nxmin, P.T.nymin, P.T.nxmax, P.T.nymax, P.T.npos, P.T.nlen};
-      void* dst[6] = {c_xmin, c_ymin, c_xmax, c_ymax, c_pos, c_len};
-      for (int a = 0; a < 6; a++)
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-                "r"(smem_addr(dst[a])),
-            "l"(src[a]), "r"(bytes), "r"(bar)
-            : "memory");
+      bulk_load(c_xmin, P.T.nxmin, bytes, bar);
+      bulk_load(c_ymin, P.T.nymin, bytes, bar);
+      bulk_load(c_xmax, P.T.nxmax, bytes, bar);
+      bulk_load(c_ymax, P.T.nymax, bytes, bar);
+      bulk_load(c_pos, P.T.npos, bytes, bar);
+      bulk_load(c_len, P.T.nlen, bytes, bar);
     }
     // bounded wait for phase 0 (twice the usual limit: after a timeout the
     // copies must not still be landing when the CTA leaves)
@@ -511,7 +375,7 @@ __global__ void __launch_bounds__(256)
     C.n = P.stage_n;
   }
 
-  int* stack = stacks + warp * P.stack_cap;
+  FrontierEntry* stack = stacks + warp * P.stack_cap;
   int lg, lc;
   lane_map(P.T.fanout, P.K, lg, lc);
   const uint32_t* order = nullptr;
@@ -709,16 +573,62 @@ static TraversalShape traversal_shape(int64_t nbox, int fanout)
   return s;
 }
 
-constexpr int kPersistThreads = 256;
+constexpr int kPersistThreads = 1024;
 constexpr int kDefaultChunk = 4096;
 constexpr int kStageMaxNodes = 2048;
 
-static int persistent_grid(size_t smem)
+// Persistent traversal variants: CTA width and CTAs per SM, which fix the
+// register budget (65536 / (threads x CTAs)).  Wider CTAs share one staged
+// copy of the top levels among more warps; narrower ones get more registers.
+struct PersistVariant {
+  int threads;
+  int min_blocks;
+  const void* fn;
+};
+
+static const PersistVariant kVariants[] = {
+    {1024, 2, (const void*)persistent_kernel<1024, 2>},  // 64 warps/SM, 32 registers
+    {512, 3, (const void*)persistent_kernel<512, 3>},    // 48 warps/SM, 40 registers
+    {256, 4, (const void*)persistent_kernel<256, 4>},    // 32 warps/SM, 64 registers
+};
+
+static const PersistVariant& variant_for(int warps_per_cta)
+{
+  for (const auto& v : kVariants)
+    if (v.threads / 32 == warps_per_cta) return v;
+  return kVariants[2];  // default: 8 warps per CTA
+}
+
+static int persistent_grid(const PersistVariant& v, size_t smem)
 {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel, kPersistThreads, smem);
+  cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, smem);
   if (per_sm < 1) per_sm = 1;
   return per_sm * sm_count();
+}
+
+// Shared memory of the persistent traversal: the staged top levels (6 arrays)
+// and one frontier stack per warp.  When that does not let the variant's CTAs
+// share an SM, staging is dropped; a stack too deep for one CTA per SM is an
+// error.
+struct PersistShape {
+  const PersistVariant* v;
+  int stage_n;
+  size_t smem;
+};
+
+static PersistShape persist_shape(int stack_cap, int stage_n, int warps_per_cta)
+{
+  const PersistVariant& v = variant_for(warps_per_cta);
+  const size_t per_sm = 227 * 1024;
+  for (int pass = 0; pass < 3; pass++) {
+    const int sn = pass == 0 ? stage_n : 0;
+    const size_t smem = (size_t)sn * 24 + (size_t)(v.threads / 32) * stack_cap * sizeof(FrontierEntry);
+    const size_t limit = pass < 2 ? per_sm / v.min_blocks - 1024 : 220 * 1024;
+    if (smem <= limit) return PersistShape{&v, sn, smem};
+  }
+  return PersistShape{nullptr, 0, 0};
 }
 
 int64_t query_capacity(int64_t pairs, const crt_query_opts& o)
@@ -726,7 +636,7 @@ int64_t query_capacity(int64_t pairs, const crt_query_opts& o)
   if (o.mode == CRT_QUERY_PLAIN) return pairs;
   const int chunk = o.chunk > 0 ? o.chunk : kDefaultChunk;
   // every resident warp may leave one partly used chunk
-  const int64_t warps = (int64_t)sm_count() * 8 * (kPersistThreads / 32);
+  const int64_t warps = (int64_t)sm_count() * 64;  // resident warps per SM at most
   return pairs + warps * chunk;
 }
 
@@ -796,13 +706,17 @@ struct TraverseLaunch {
   PersistParams P;
   size_t smem;
   int grid;
+  int threads;
+  const void* fn;
 };
 
 static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
                                     const PersistScratch& S, bool sort, int stage_n,
-                                    int32_t* fid, int32_t* tid, long long cap, int chunk)
+                                    int32_t* fid, int32_t* tid, long long cap, int chunk,
+                                    int warps_per_cta)
 {
   const TraversalShape sh = traversal_shape(T.nbox, T.fanout);
+  const PersistShape ps = persist_shape(sh.stack_cap, stage_n, warps_per_cta);
   TraverseLaunch L;
   PersistParams& P = L.P;
   P.T = T;
@@ -812,7 +726,7 @@ static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
   P.sort_ctrl = sort ? sort_ctrl(S.sort_zero) : nullptr;
   P.K = sh.K;
   P.stack_cap = sh.stack_cap;
-  P.stage_n = stage_n;
+  P.stage_n = ps.stage_n;
   P.chunk = chunk;
   P.fid = fid;
   P.tid = tid;
@@ -820,16 +734,18 @@ static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
   P.ctr = S.ctr;
   P.holes = S.holes;
   P.max_holes = S.max_holes;
-  L.smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
-  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem);
-  L.grid = persistent_grid(L.smem);
+  L.smem = ps.smem;
+  L.threads = ps.v->threads;
+  L.fn = ps.v->fn;
+  L.grid = persistent_grid(*ps.v, L.smem);
   return L;
 }
 
 static void launch_traverse(const TraverseLaunch& L, cudaStream_t stream)
 {
   ProfScope ps("traverse_persistent", stream);
-  persistent_kernel<<<L.grid, kPersistThreads, L.smem, stream>>>(L.P);
+  void* args[] = {(void*)&L.P};
+  cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.threads), args, L.smem, stream);
   CRT_LAUNCHED(1);
 }
 
@@ -856,9 +772,10 @@ static int stage_nodes_for(const crt_rtree_f32& rt, bool want)
   return n & ~3;
 }
 
-static long long max_holes_for(size_t smem)
+static long long max_holes_for(int stack_cap, int stage_n, int warps_per_cta)
 {
-  return (long long)persistent_grid(smem) * (kPersistThreads / 32);
+  const PersistShape ps = persist_shape(stack_cap, stage_n, warps_per_cta);
+  return (long long)persistent_grid(*ps.v, ps.smem) * (ps.v->threads / 32);
 }
 
 int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
@@ -892,7 +809,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
     long long* offsets = d_offsets ? (long long*)d_offsets : sums + nb + 32;
     cudaMemsetAsync(ctr, 0, sizeof(QueryCounters), stream);
     cudaMemsetAsync(offsets, 0, 8, stream);
-    const size_t smem = (size_t)kPlainWarps * sh.stack_cap * 4;
+    const size_t smem = (size_t)kPlainWarps * sh.stack_cap * sizeof(FrontierEntry);
     cudaFuncSetAttribute(plain_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(plain_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (nq > 0) {
@@ -924,10 +841,9 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   const bool sort = opts.sort_windows != 0 && nq > 1;
   const int stage_n = stage_nodes_for(rt, opts.stage_levels != 0);
   const int chunk = opts.chunk >= 64 ? opts.chunk : kDefaultChunk;
-  const size_t smem = (size_t)stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
-  if (smem > 200 * 1024) return fail(CRT_ERR_NOT_SUPPORTED, "query: traversal stack too large");
-  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const long long max_holes = max_holes_for(smem);
+  if (!persist_shape(sh.stack_cap, stage_n, opts.warps_per_cta).v)
+    return fail(CRT_ERR_NOT_SUPPORTED, "query: traversal stack too large");
+  const long long max_holes = max_holes_for(sh.stack_cap, stage_n, opts.warps_per_cta);
   const size_t bytes = persist_scratch_bytes(nq, max_holes, sort);
   char* scr = nullptr;
   if (cudaMallocAsync((void**)&scr, bytes, stream) != cudaSuccess) {
@@ -939,7 +855,9 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   set_nq_kernel<<<1, 1, 0, stream>>>(S.ctr, nq);
   CRT_LAUNCHED(1);
   enqueue_pre(W, nq, S, sort, stream);
-  launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk), stream);
+  launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk,
+                                opts.warps_per_cta),
+                  stream);
   enqueue_post(S, fid, tid, capacity, d_result, stream);
   cudaFreeAsync(scr, stream);
   cudaError_t e = cudaGetLastError();
@@ -962,7 +880,7 @@ int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   QueryCounters* ctr = (QueryCounters*)scr;
   unsigned long long* tot = (unsigned long long*)(scr + 256);
   cudaMemsetAsync(scr, 0, 512, stream);
-  const size_t smem = (size_t)kPlainWarps * sh.stack_cap * 4;
+  const size_t smem = (size_t)kPlainWarps * sh.stack_cap * sizeof(FrontierEntry);
   cudaFuncSetAttribute(stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (qbox.sz > 0) {
     stats_kernel<<<(unsigned)cdiv(qbox.sz, kPlainWarps), kPlainWarps * 32, smem, stream>>>(
@@ -1025,9 +943,11 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   p->cap = capacity;
   p->res = res;
   const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
-  const size_t smem = (size_t)p->stage_n * 24 + (size_t)(kPersistThreads / 32) * sh.stack_cap * 4;
-  cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const long long max_holes = max_holes_for(smem);
+  if (!persist_shape(sh.stack_cap, p->stage_n, opts.warps_per_cta).v) {
+    delete p;
+    return fail(CRT_ERR_NOT_SUPPORTED, "plan: traversal stack too large");
+  }
+  const long long max_holes = max_holes_for(sh.stack_cap, p->stage_n, opts.warps_per_cta);
   const size_t bytes = persist_scratch_bytes(max_nq, max_holes, p->sort);
   if (cudaMalloc((void**)&p->scratch, bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -1037,7 +957,8 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   persist_scratch_carve(p->scratch, max_nq, max_holes, p->sort, p->S);
   cudaMemsetAsync(p->S.ctr, 0, sizeof(QueryCounters), stream);
   set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
-  p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk);
+  p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk,
+                              opts.warps_per_cta);
   // capture pre and post on a private stream
   cudaStream_t cs;
   if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {

@@ -216,6 +216,68 @@ int crt_plan_launch(crt_plan plan, crt_stream_t stream);
 int crt_plan_destroy(crt_plan plan);
 
 /* ---------------------------------------------------------------------- */
+/* Serving loop (no reference counterpart: the reference answers one batch   */
+/* per call)                                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* Continuous batching of window-query requests against device-resident
+ * trees.  One persistent kernel serves every admitted request; requests that
+ * arrive while others run are admitted as soon as a request slot and arena
+ * memory are free, and their windows are processed alongside the others'.
+ * A request is admitted by its HBM footprint: 16 bytes per window plus an
+ * output estimate of 8 bytes per expected pair (running pairs-per-window
+ * average of its tree times output_slack).  A request whose output outgrows
+ * the estimate is re-run with its exact size (overflow-and-retry) before it
+ * completes.  Results stay in the arena until crt_server_release. */
+typedef struct crt_server_s* crt_server;
+
+typedef struct {
+  int64_t arena_bytes;     /* device memory for windows and outputs in flight (default 8 GiB) */
+  int max_requests;        /* request slots admitted at once (default 4096) */
+  int max_trees;           /* default 16 */
+  double pairs_per_window; /* initial output estimate per window (default 64) */
+  double output_slack;     /* multiplier on the estimate (default 1.5, >= 1) */
+  int idle_ms;             /* stop the device loop after this long without work (default 20) */
+  int64_t device_wait_us;  /* bound on any device-side wait (default 2 s) */
+  int reserved[4];
+} crt_server_opts;
+
+typedef struct {
+  int64_t request_id;
+  int tree_id;
+  int status;           /* CRT_OK, or the error that ended the request */
+  int64_t nq;
+  int64_t count;        /* hit pairs */
+  int32_t* d_fid;       /* device, count entries: box ids */
+  int32_t* d_tid;       /* device, count entries: window index within the request */
+  double submit_time_s; /* steady clock, seconds */
+  double complete_time_s;
+  int retries;          /* overflow re-runs */
+  int reserved;
+} crt_server_completion;
+
+void crt_server_opts_default(crt_server_opts* o);
+int crt_server_create(const crt_server_opts* opts, crt_server* out);
+/* Registers a built tree (crt_build_f32 output: d_rbox is the sorted box set).
+ * The arrays must outlive the server.  Trees are added before the first
+ * submission. */
+int crt_server_add_tree(crt_server s, const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                        int* tree_id);
+/* Admits nq windows (host or device pointers; copied before return) for one
+ * tree, or returns CRT_ERR_BUSY when no slot or arena space is free now. */
+int crt_server_submit(crt_server s, int tree_id, const float* xmin, const float* ymin,
+                      const float* xmax, const float* ymax, int64_t nq, int64_t* request_id);
+/* Takes up to max_out completions, waiting up to wait_ms for the first. */
+int crt_server_poll(crt_server s, crt_server_completion* out, int max_out, int* n_out,
+                    int wait_ms);
+/* Frees a completed request's windows and output. */
+int crt_server_release(crt_server s, int64_t request_id);
+/* Counters; returns the device loop's last error status (CRT_OK if none). */
+int crt_server_stats(crt_server s, int64_t* submitted, int64_t* completed, int64_t* retried,
+                     int64_t* arena_used);
+int crt_server_destroy(crt_server s);
+
+/* ---------------------------------------------------------------------- */
 /* Kernel timing (no reference counterpart; the reference prints host        */
 /* gettimeofday timers, src/rtree_bulkload_thrust.cuh:74-89)                */
 /* ---------------------------------------------------------------------- */

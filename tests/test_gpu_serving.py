@@ -1,0 +1,159 @@
+"""Serving loop on the GPU (continuous batching through one persistent kernel):
+each request's result is the same in the mix as alone, requests admitted by
+HBM footprint, undersized outputs re-run with their exact size, and a
+device-side wait that runs out is reported as a status without harming the
+context."""
+import time
+
+import numpy as np
+import pytest
+
+from curtree_b200 import datasets as D
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import curtree_b200 as C
+    from curtree_b200.server import Server
+    trees = []
+    for i, (n, f) in enumerate([(200_000, 10), (500_000, 16), (1_000_000, 8)]):
+        b = D.uniform_boxes(n, seed=70 + i)
+        d = C.BBox.from_host(b)
+        rt = C.RTree(f)
+        C.build_rtree(d, rt)
+        sb, t = O.build(b, f)
+        trees.append({"rt": rt, "d": d, "sb": sb, "t": t, "f": f})
+    return C, Server, trees
+
+
+def make_requests(trees, n_req, seed, max_windows=3000):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n_req):
+        ti = int(rng.integers(0, len(trees)))
+        nq = int(np.exp(rng.uniform(0, np.log(max_windows))))
+        w = D.mixed_windows(nq, trees[ti]["sb"], seed=1000 * seed + i, lo=1e-5, hi=3e-2)
+        reqs.append((ti, w))
+    return reqs
+
+
+def expected(trees, ti, w):
+    t = trees[ti]
+    return O.canonical_pairs(*O.tree_query_pairs(t["t"], t["sb"], w))
+
+
+def run_all(srv, tree_ids, reqs, timeout_s=120):
+    ids = {}
+    done = {}
+    queue = list(range(len(reqs)))
+    t0 = time.monotonic()
+    while (queue or len(done) < len(reqs)) and time.monotonic() - t0 < timeout_s:
+        while queue:
+            i = queue[0]
+            rid = srv.submit(tree_ids[reqs[i][0]], reqs[i][1])
+            if rid is None:
+                break
+            ids[rid] = i
+            queue.pop(0)
+        for c in srv.poll(max_out=64, wait_ms=5):
+            i = ids[c["request_id"]]
+            done[i] = (c, srv.pairs(c))
+            srv.release(c["request_id"])
+    assert not queue and len(done) == len(reqs), "requests did not complete"
+    return done
+
+
+def setup_server(C, Server, trees, **kw):
+    srv = Server(**kw)
+    ids = [srv.add_tree(t["rt"], t["d"]) for t in trees]
+    return srv, ids
+
+
+def test_results_same_alone_and_in_the_mix(env):
+    C, Server, trees = env
+    srv, ids = setup_server(C, Server, trees, arena_bytes=2 << 30)
+    reqs = make_requests(trees, 80, seed=1)
+    done = run_all(srv, ids, reqs)
+    for i, (ti, w) in enumerate(reqs):
+        c, (fid, tid) = done[i]
+        assert c["status"] == 0
+        got = O.canonical_pairs(fid, tid)
+        want = expected(trees, ti, w)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), i
+        # alone: the same request through the plain per-batch form
+        dq = C.BBox.from_host(w)
+        pf, pt, _ = C.query(trees[ti]["rt"], trees[ti]["d"], dq, mode=C.CRT_QUERY_PLAIN)
+        alone = O.canonical_pairs(pf.cpu().numpy(), pt.cpu().numpy())
+        assert np.array_equal(alone[0], got[0]) and np.array_equal(alone[1], got[1])
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["arena_used"] == 0
+    assert srv.close() == 0
+
+
+def test_overflow_and_retry(env):
+    C, Server, trees = env
+    srv, ids = setup_server(C, Server, trees, pairs_per_window=0.01, output_slack=1.0)
+    reqs = make_requests(trees, 25, seed=2)
+    done = run_all(srv, ids, reqs)
+    retried = sum(done[i][0]["retries"] for i in done)
+    assert retried > 0 and srv.stats()["retried"] == retried
+    for i, (ti, w) in enumerate(reqs):
+        got = O.canonical_pairs(*done[i][1])
+        want = expected(trees, ti, w)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), i
+    srv.close()
+
+
+def test_admission_by_footprint(env):
+    C, Server, trees = env
+    # room for about one request of this size at a time
+    srv, ids = setup_server(C, Server, trees, arena_bytes=4 << 20, pairs_per_window=50.0)
+    w = D.mixed_windows(4000, trees[0]["sb"], seed=77, lo=1e-5, hi=1e-3)
+    a = srv.submit(ids[0], w)
+    assert a is not None
+    b = srv.submit(ids[0], w)
+    assert b is None, "a second request must wait for arena space"
+    cs = []
+    t0 = time.monotonic()
+    while not cs and time.monotonic() - t0 < 30:
+        cs = srv.poll(wait_ms=10)
+    assert cs and cs[0]["request_id"] == a
+    srv.release(a)
+    assert srv.submit(ids[0], w) is not None
+    srv.close()
+
+
+def test_device_wait_timeout_is_reported(env):
+    """The idle device loop's bounded wait runs out (no work is published and
+    the host does not stop it for 10 s): the kernel records
+    CRT_ERR_DEVICE_TIMEOUT and returns; the host reads the status and later
+    requests still run."""
+    C, Server, trees = env
+    srv, ids = setup_server(C, Server, trees, idle_ms=10_000, device_wait_us=5_000)
+    w = D.mixed_windows(500, trees[1]["sb"], seed=78, lo=1e-5, hi=1e-2)
+    rid = srv.submit(ids[1], w)
+    cs = []
+    t0 = time.monotonic()
+    while not cs and time.monotonic() - t0 < 30:
+        cs = srv.poll(wait_ms=10)
+    assert cs and cs[0]["status"] == 0
+    srv.release(rid)
+    time.sleep(0.3)
+    assert srv.stats()["device_status"] == C._lib.CRT_ERR_DEVICE_TIMEOUT
+    # the context is intact: another request runs to completion, exactly
+    rid = srv.submit(ids[1], w)
+    cs = []
+    t0 = time.monotonic()
+    while not cs and time.monotonic() - t0 < 30:
+        cs = srv.poll(wait_ms=10)
+    assert cs and cs[0]["status"] == 0
+    got = O.canonical_pairs(*Server.pairs(cs[0]))
+    want = expected(trees, 1, w)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    srv.release(rid)
+    srv.close()
