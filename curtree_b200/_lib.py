@@ -50,7 +50,8 @@ class crt_idpair(ctypes.Structure):
 class crt_query_opts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("sort_windows", ctypes.c_int),
                 ("stage_levels", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
-                ("chunk", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("chunk", ctypes.c_int), ("no_contain", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class crt_query_result(ctypes.Structure):

@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "internal.h"
@@ -62,6 +63,7 @@ struct CountEmit {
   long long hits = 0;
   __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
+  __device__ __forceinline__ void range(const int*, long long, long long count) { hits += count; }
 };
 
 // Counts hits and the leaf boxes tested (workload statistics).
@@ -72,6 +74,7 @@ struct StatEmit {
   __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
   __device__ __forceinline__ void leaf_tests(int n) { tested += n; }
+  __device__ __forceinline__ void range(const int*, long long, long long count) { hits += count; }
 };
 
 // Writes at precomputed per-window offsets (plain write pass).
@@ -93,6 +96,18 @@ struct OffsetEmit {
       tid[slot] = q;
     }
     base += __popc(m);
+  }
+  __device__ __forceinline__ void range(const int* bid, long long first, long long count)
+  {
+    const int lane = (int)lane_id();
+    for (long long i = lane; i < count; i += 32) {
+      const long long slot = base + i;
+      if (slot < cap) {
+        fid[slot] = __ldg(bid + first + i);
+        tid[slot] = q;
+      }
+    }
+    base += count;
   }
 };
 
@@ -131,6 +146,26 @@ struct ChunkEmit {
     if (hit && slot < cap) {
       fid[slot] = id;
       tid[slot] = q;
+    }
+  }
+  // A contained subtree's ids are copied to an exact reservation of their
+  // own (no unused chunk end); short ranges go through the chunk.
+  __device__ __forceinline__ void range(const int* bid, long long first, long long count)
+  {
+    if (count < 256) {
+      emit_range_default(*this, bid, first, count);
+      return;
+    }
+    unsigned long long nb = 0;
+    if (lane_id() == 0) nb = atomicAdd(next, (unsigned long long)count);
+    nb = __shfl_sync(0xffffffffu, nb, 0);
+    hits += count;
+    for (long long i = lane_id(); i < count; i += 32) {
+      const long long slot = (long long)nb + i;
+      if (slot < cap) {
+        fid[slot] = __ldg(bid + first + i);
+        tid[slot] = q;
+      }
     }
   }
 };
@@ -188,8 +223,8 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
   lane_map(T.fanout, K, lg, lc);
   NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   StatEmit emit;
-  traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
-           s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
+  traverse<StatEmit, false>(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
+                            s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
   if (lane_id() == 0) {
     if (hits) hits[q] = emit.hits;
     if (tested) tested[q] = emit.tested;
@@ -545,7 +580,48 @@ static TreeView make_view(const crt_rtree_f32& rt, const crt_bbox_f32& rb)
   T.npos = rt.pos; T.nlen = rt.len; T.rsz = rt.sz; T.fanout = rt.fanout;
   T.bxmin = rb.xmin; T.bymin = rb.ymin; T.bxmax = rb.xmax; T.bymax = rb.ymax; T.bid = rb.id;
   T.nbox = rb.sz;
+  T.nlev = 0;
+  T.lvl_first = nullptr;
+  T.lvl_span = nullptr;
   return T;
+}
+
+// The tables hold only for the reference's packed layout, which a tree has
+// exactly when its node count is the packed count for its box count.
+LevelTables level_tables(const crt_rtree_f32& rt, int64_t nbox)
+{
+  LevelTables t;
+  if (rt.sz <= 0 || rt.fanout < 2 || rt.fanout > kLenMask) return t;
+  std::vector<int64_t> lv;
+  const int L = tree_levels(nbox, rt.fanout, lv);
+  if (L <= 0 || L > kMaxLevels) return t;
+  int64_t rsz = 0;
+  for (auto x : lv) rsz += x;
+  if (rsz != rt.sz) return t;
+  int64_t start = rsz;
+  long long sp = rt.fanout;
+  for (int h = 0; h < L; h++) {
+    start -= lv[h];
+    t.first[h] = (int)start;
+    t.span[h] = sp;
+    sp = sp > (1ll << 40) ? sp : sp * rt.fanout;
+  }
+  t.nlev = L;
+  return t;
+}
+
+// Uploads the tables to `dev` (kLevelTableBytes, 8-byte aligned) and points
+// the view at them.
+static void attach_levels(TreeView& T, const LevelTables& t, void* dev, cudaStream_t stream)
+{
+  if (t.nlev == 0) return;
+  char buf[kLevelTableBytes];
+  std::memcpy(buf, t.first, sizeof(int) * kMaxLevels);
+  std::memcpy(buf + sizeof(int) * kMaxLevels, t.span, sizeof(long long) * kMaxLevels);
+  cudaMemcpyAsync(dev, buf, kLevelTableBytes, cudaMemcpyHostToDevice, stream);
+  T.nlev = t.nlev;
+  T.lvl_first = (const int*)dev;
+  T.lvl_span = (const long long*)((char*)dev + sizeof(int) * kMaxLevels);
 }
 
 // Number of levels of a tree with R_sz nodes over nbox boxes at this fanout
@@ -573,7 +649,6 @@ static TraversalShape traversal_shape(int64_t nbox, int fanout)
   return s;
 }
 
-constexpr int kPersistThreads = 1024;
 constexpr int kDefaultChunk = 4096;
 constexpr int kStageMaxNodes = 2048;
 
@@ -787,7 +862,8 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
     return fail(CRT_ERR_INVALID_ARG, "query: negative size");
   if (rt.sz > 0 && rt.fanout < 2) return fail(CRT_ERR_INVALID_ARG, "query: fanout < 2");
   if (capacity > 0 && (!fid || !tid)) return fail(CRT_ERR_INVALID_ARG, "query: null output");
-  const TreeView T = make_view(rt, rbox);
+  TreeView T = make_view(rt, rbox);
+  const LevelTables lt = opts.no_contain ? LevelTables() : level_tables(rt, rbox.sz);
   WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};
   const int64_t nq = qbox.sz;
   const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
@@ -797,7 +873,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
     // scratch: counters, counts, block sums (+ offsets when the caller gave none)
     const int64_t nb = std::max<int64_t>(1, cdiv(nq, kScanThreads));
     size_t bytes = 256 + 8 * (size_t)std::max<int64_t>(nq, 1) + 8 * (size_t)nb + 256 +
-                   (d_offsets ? 0 : 8 * (size_t)(nq + 1) + 256);
+                   (d_offsets ? 0 : 8 * (size_t)(nq + 1) + 256) + kLevelTableBytes + 256;
     char* scr = nullptr;
     if (cudaMallocAsync((void**)&scr, bytes, stream) != cudaSuccess) {
       cudaGetLastError();
@@ -807,6 +883,8 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
     long long* counts = (long long*)(scr + 256);
     long long* sums = counts + std::max<int64_t>(nq, 1);
     long long* offsets = d_offsets ? (long long*)d_offsets : sums + nb + 32;
+    char* tables = (char*)(((uintptr_t)(scr + bytes - kLevelTableBytes - 256) + 255) & ~(uintptr_t)255);
+    attach_levels(T, lt, tables, stream);
     cudaMemsetAsync(ctr, 0, sizeof(QueryCounters), stream);
     cudaMemsetAsync(offsets, 0, 8, stream);
     const size_t smem = (size_t)kPlainWarps * sh.stack_cap * sizeof(FrontierEntry);
@@ -844,7 +922,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   if (!persist_shape(sh.stack_cap, stage_n, opts.warps_per_cta).v)
     return fail(CRT_ERR_NOT_SUPPORTED, "query: traversal stack too large");
   const long long max_holes = max_holes_for(sh.stack_cap, stage_n, opts.warps_per_cta);
-  const size_t bytes = persist_scratch_bytes(nq, max_holes, sort);
+  const size_t bytes = persist_scratch_bytes(nq, max_holes, sort) + kLevelTableBytes;
   char* scr = nullptr;
   if (cudaMallocAsync((void**)&scr, bytes, stream) != cudaSuccess) {
     cudaGetLastError();
@@ -852,6 +930,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   }
   PersistScratch S;
   persist_scratch_carve(scr, nq, max_holes, sort, S);
+  attach_levels(T, lt, scr + S.bytes, stream);
   set_nq_kernel<<<1, 1, 0, stream>>>(S.ctr, nq);
   CRT_LAUNCHED(1);
   enqueue_pre(W, nq, S, sort, stream);
@@ -948,13 +1027,14 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
     return fail(CRT_ERR_NOT_SUPPORTED, "plan: traversal stack too large");
   }
   const long long max_holes = max_holes_for(sh.stack_cap, p->stage_n, opts.warps_per_cta);
-  const size_t bytes = persist_scratch_bytes(max_nq, max_holes, p->sort);
+  const size_t bytes = persist_scratch_bytes(max_nq, max_holes, p->sort) + kLevelTableBytes;
   if (cudaMalloc((void**)&p->scratch, bytes) != cudaSuccess) {
     cudaGetLastError();
     delete p;
     return fail(CRT_ERR_OOM, "plan: scratch allocation failed");
   }
   persist_scratch_carve(p->scratch, max_nq, max_holes, p->sort, p->S);
+  if (!opts.no_contain) attach_levels(p->T, level_tables(rt, rbox.sz), p->scratch + p->S.bytes, stream);
   cudaMemsetAsync(p->S.ctr, 0, sizeof(QueryCounters), stream);
   set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
   p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk,

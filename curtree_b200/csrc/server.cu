@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -61,6 +62,9 @@ struct SrvTree {
   int fanout;
   int nbox;
   int K;
+  int nlev;  // containment tables (nlev == 0: off)
+  const int* lvl_first;
+  const long long* lvl_span;
 };
 
 struct SrvDesc {
@@ -136,6 +140,24 @@ struct StagedEmit {
     __syncwarp();
   }
   __device__ __forceinline__ void begin(int qq) { q = qq; }
+  // A contained subtree's ids go straight to an exact reservation.
+  __device__ __forceinline__ void range(const int* bid, long long first, long long count)
+  {
+    if (count < kStage) {
+      emit_range_default(*this, bid, first, count);
+      return;
+    }
+    unsigned long long b = 0;
+    if (lane_id() == 0) b = atomicAdd(&ctr->next, (unsigned long long)count);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    for (long long i = lane_id(); i < count; i += 32) {
+      const long long slot = (long long)b + i;
+      if (slot < cap) {
+        fid[slot] = __ldg(bid + first + i);
+        tid[slot] = q;
+      }
+    }
+  }
   __device__ __forceinline__ void operator()(bool hit, int id)
   {
     const uint32_t m = __ballot_sync(0xffffffffu, hit);
@@ -220,6 +242,7 @@ __global__ void __launch_bounds__(kSrvThreads)
     T.npos = tr.npos; T.nlen = tr.nlen; T.rsz = tr.rsz; T.fanout = tr.fanout;
     T.bxmin = tr.bxmin; T.bymin = tr.bymin; T.bxmax = tr.bxmax; T.bymax = tr.bymax;
     T.bid = tr.bid; T.nbox = tr.nbox;
+    T.nlev = tr.nlev; T.lvl_first = tr.lvl_first; T.lvl_span = tr.lvl_span;
     int lg, lc;
     lane_map(T.fanout, tr.K, lg, lc);
     SrvCtr* ctr = &ctrs[r % slots];
@@ -317,6 +340,15 @@ struct Request {
   long long seq = -1;  // sequence number while published
   double t_submit = 0;
   int retries = 0;
+  double predicted = 0;  // area-based pair estimate (0: none)
+};
+
+// Host-side statistics of a tree for output estimates.
+struct TreeStats {
+  double rx1 = 0, ry1 = 0, rx2 = 0, ry2 = 0;  // root MBR
+  double density = 0;                          // boxes per unit area
+  double mbw = 0, mbh = 0;                     // mean box extents (sample)
+  double corr = 1.0;                           // EMA of actual / predicted pairs
 };
 
 }  // namespace
@@ -331,7 +363,10 @@ struct Server {
   // device tables
   SrvTree* d_trees = nullptr;
   std::vector<SrvTree> trees;
+  std::vector<char*> tables;  // containment tables, one allocation per tree
   std::vector<double> tree_ppw;  // pairs per window estimate per tree
+  std::vector<TreeStats> tree_stats;
+  std::deque<Request> retry_wait;  // re-runs waiting for arena space
   SrvDesc* d_descs = nullptr;
   SrvCtr* d_ctrs = nullptr;
   SrvState* d_state = nullptr;
@@ -436,6 +471,33 @@ struct Server {
     cudaStreamSynchronize(copy);
   }
 
+  // Expected pairs of a window batch against a tree: windows clipped to the
+  // tree's root MBR and grown by the mean box extents, times the box density,
+  // times the tree's learned correction.
+  double predict_locked(int tree, const float* x1, const float* y1, const float* x2,
+                        const float* y2, long long nq) const
+  {
+    const TreeStats& t = tree_stats[tree];
+    if (t.density <= 0) return 0;
+    double sum = 0;
+    for (long long i = 0; i < nq; i++) {
+      const double w = std::min<double>(x2[i] + t.mbw, t.rx2) - std::max<double>(x1[i] - t.mbw, t.rx1);
+      const double h = std::min<double>(y2[i] + t.mbh, t.ry2) - std::max<double>(y1[i] - t.mbh, t.ry1);
+      if (w > 0 && h > 0) sum += w * h;
+    }
+    return sum * t.density;
+  }
+
+  void learn_locked(const Request& q, long long count)
+  {
+    tree_ppw[q.tree] = 0.8 * tree_ppw[q.tree] + 0.2 * ((double)count / std::max(1LL, q.nq));
+    if (q.predicted > 0) {
+      TreeStats& t = tree_stats[q.tree];
+      const double r = std::min(16.0, std::max(1.0 / 16, (double)count / q.predicted));
+      t.corr = 0.7 * t.corr + 0.3 * r;
+    }
+  }
+
   void finish_locked(Request& q, long long count, int status)
   {
     crt_server_completion c{};
@@ -466,26 +528,26 @@ struct Server {
         if (h_done[slot].seq == q.seq) {
           const long long count = h_done[slot].count;
           progressed = true;
+          learn_locked(q, count);
           if (count > q.cap) {
-            // overflow-and-retry: rerun with the exact size
+            // overflow-and-retry: re-run with the exact size once the arena
+            // has room for it
             n_retried++;
             alloc.release(q.out_off, q.out_bytes);
-            size_t off;
             Request rq = q;
             rq.cap = count;
             rq.out_bytes = (size_t)count * 8;
+            rq.out_off = 0;
             rq.retries++;
-            if (alloc.alloc(rq.out_bytes, off)) {
-              rq.out_off = off;
-              rq.seq = -1;
-              pending.push_back(rq);
-            } else {
+            rq.seq = -1;
+            if (rq.out_bytes + rq.win_bytes > arena_bytes) {
               rq.out_bytes = 0;
               rq.cap = 0;
               finish_locked(rq, count, CRT_ERR_OOM);
+            } else {
+              retry_wait.push_back(rq);
             }
           } else {
-            tree_ppw[q.tree] = 0.8 * tree_ppw[q.tree] + 0.2 * ((double)count / std::max(1LL, q.nq));
             finish_locked(q, count, CRT_OK);
           }
           it = flight.erase(it);
@@ -500,6 +562,15 @@ struct Server {
       } else {
         oldest_seq = next_seq;
       }
+      // re-runs waiting for arena space, oldest first
+      while (!retry_wait.empty()) {
+        size_t off;
+        if (!alloc.alloc(retry_wait.front().out_bytes, off)) break;
+        Request rq = retry_wait.front();
+        retry_wait.pop_front();
+        rq.out_off = off;
+        pending.push_back(rq);
+      }
       if (progressed) cv.notify_all();
       if (!pending.empty()) {
         if (!kernel_running) launch_kernel();
@@ -507,7 +578,7 @@ struct Server {
         last_work = now_s();
       }
       if (!flight.empty()) last_work = now_s();
-      if (kernel_running && flight.empty() && pending.empty() &&
+      if (kernel_running && flight.empty() && pending.empty() && retry_wait.empty() &&
           now_s() - last_work > opts.idle_ms * 1e-3) {
         lk.unlock();
         stop_kernel();
@@ -585,7 +656,7 @@ int crt_server_create(const crt_server_opts* opts, crt_server* out)
     delete s;
     return fail(CRT_ERR_INVALID_ARG, "server_create: bad options");
   }
-  if (o.output_slack < 1.0) o.output_slack = 1.0;
+  if (!(o.output_slack > 0)) o.output_slack = 1.5;
   cudaGetDevice(&s->device);
   s->slots = o.max_requests;
   s->arena_bytes = (size_t)o.arena_bytes;
@@ -650,8 +721,49 @@ int crt_server_add_tree(crt_server h, const crt_rtree_f32* rt, const crt_bbox_f3
   int cap = ((L - 1) * t.K * std::max(2, rt->fanout) + 1 + 31) / 32 * 32;
   s->stack_cap = std::max(s->stack_cap, cap);
   if (s->smem() > 200 * 1024) return fail(CRT_ERR_NOT_SUPPORTED, "server_add_tree: tree too deep");
+  const LevelTables lt = level_tables(*rt, rbox->sz);
+  t.nlev = 0;
+  if (lt.nlev > 0) {
+    char* dev = nullptr;
+    if (cudaMalloc((void**)&dev, kLevelTableBytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(CRT_ERR_OOM, "server_add_tree: table allocation failed");
+    }
+    cudaMemcpy(dev, lt.first, sizeof(int) * kMaxLevels, cudaMemcpyHostToDevice);
+    cudaMemcpy(dev + sizeof(int) * kMaxLevels, lt.span, sizeof(long long) * kMaxLevels,
+               cudaMemcpyHostToDevice);
+    s->tables.push_back(dev);
+    t.nlev = lt.nlev;
+    t.lvl_first = (const int*)dev;
+    t.lvl_span = (const long long*)(dev + sizeof(int) * kMaxLevels);
+  }
+  TreeStats ts;
+  if (rt->sz > 0 && rbox->sz > 0) {
+    // root MBR and a sample of box extents
+    float root[4];
+    const float* src[4] = {rt->xmin, rt->ymin, rt->xmax, rt->ymax};
+    for (int a = 0; a < 4; a++) cudaMemcpy(&root[a], src[a], sizeof(float), cudaMemcpyDeviceToHost);
+    const int m = std::min(rbox->sz, 4096);
+    std::vector<float> bx[4];
+    const float* bs[4] = {rbox->xmin, rbox->ymin, rbox->xmax, rbox->ymax};
+    for (int a = 0; a < 4; a++) {
+      bx[a].resize(m);
+      cudaMemcpy(bx[a].data(), bs[a], sizeof(float) * m, cudaMemcpyDeviceToHost);
+    }
+    double sw = 0, sh = 0;
+    for (int i = 0; i < m; i++) {
+      if (bx[2][i] >= bx[0][i]) sw += bx[2][i] - bx[0][i];
+      if (bx[3][i] >= bx[1][i]) sh += bx[3][i] - bx[1][i];
+    }
+    ts.rx1 = root[0]; ts.ry1 = root[1]; ts.rx2 = root[2]; ts.ry2 = root[3];
+    const double area = (ts.rx2 - ts.rx1) * (ts.ry2 - ts.ry1);
+    ts.density = area > 0 && std::isfinite(area) ? rbox->sz / area : 0;
+    ts.mbw = sw / m;
+    ts.mbh = sh / m;
+  }
   const int id = (int)s->trees.size();
   s->trees.push_back(t);
+  s->tree_stats.push_back(ts);
   s->tree_ppw.push_back(s->opts.pairs_per_window);
   cudaError_t e = cudaMemcpy(s->d_trees + id, &t, sizeof(t), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cuda_fail(e, "server_add_tree");
@@ -676,8 +788,15 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
     q.tree = tree_id;
     q.nq = nq;
     q.win_bytes = (size_t)nq * 16;
-    const double est = s->tree_ppw[tree_id] * (double)nq * s->opts.output_slack + 256.0;
-    q.cap = (long long)est;
+    cudaPointerAttributes pa{};
+    const bool host_windows = cudaPointerGetAttributes(&pa, xmin) == cudaSuccess &&
+                              pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged;
+    cudaGetLastError();
+    q.predicted = host_windows ? s->predict_locked(tree_id, xmin, ymin, xmax, ymax, nq) : 0;
+    const double est = q.predicted > 0
+                           ? s->tree_stats[tree_id].corr * q.predicted * s->opts.output_slack + 256.0
+                           : s->tree_ppw[tree_id] * (double)nq * s->opts.output_slack + 256.0;
+    q.cap = (long long)std::min(est, 4.0e12);
     q.out_bytes = (size_t)q.cap * 8;
     if (!s->alloc.alloc(q.win_bytes, q.win_off))
       return fail(CRT_ERR_BUSY, "server_submit: arena full (windows)");
@@ -761,6 +880,7 @@ int crt_server_destroy(crt_server h)
   if (s->worker.joinable()) s->worker.join();
   if (s->compute) cudaStreamSynchronize(s->compute);
   cudaFree(s->arena);
+  for (char* t : s->tables) cudaFree(t);
   cudaFree(s->d_trees);
   cudaFree(s->d_descs);
   cudaFree(s->d_ctrs);

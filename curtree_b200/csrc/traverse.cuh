@@ -22,6 +22,10 @@
 
 namespace crt {
 
+// Deepest tree the containment shortcut handles (a tree of 2^31 boxes at
+// fanout 2 has 31 levels).
+constexpr int kMaxLevels = 40;
+
 struct TreeView {
   const float* __restrict__ nxmin;
   const float* __restrict__ nymin;
@@ -37,7 +41,25 @@ struct TreeView {
   const float* __restrict__ bymax;
   const int* __restrict__ bid;
   int nbox;
+  // Packed-layout tables for the containment shortcut (nlev == 0: off).  In
+  // the reference's bulk-load layout the subtree of the g-th node of height h
+  // (h = 0: leaf-parents) holds the sorted slots
+  // [g * span[h], min(nbox, (g + 1) * span[h])), span[h] = fanout^(h + 1).
+  int nlev;
+  const int* __restrict__ lvl_first;        // first node index of height h
+  const long long* __restrict__ lvl_span;   // boxes under a full node of height h
 };
+
+// Host image of the containment tables: kMaxLevels ints (first node of each
+// height) then kMaxLevels int64 (boxes under a full node of that height).
+struct LevelTables {
+  int nlev = 0;
+  int first[kMaxLevels];
+  long long span[kMaxLevels];
+};
+constexpr size_t kLevelTableBytes = sizeof(int) * kMaxLevels + sizeof(long long) * kMaxLevels;
+// Tables of a tree in the reference's packed layout; nlev == 0 otherwise.
+LevelTables level_tables(const crt_rtree_f32& rt, int64_t nbox);
 
 struct WindowView {
   const float* __restrict__ xmin;
@@ -83,9 +105,27 @@ __device__ __forceinline__ void load_node_link(const TreeView& T, const NodeCach
 // One frontier entry: the children range [pos, pos + len) of a node that
 // intersected the window.  Carrying the range on the stack (it is loaded with
 // the node's MBR when the node is tested) saves a dependent load per level.
+// With the containment shortcut on, the high 8 bits of `len` hold the height
+// of the nodes in the range.
 typedef int2 FrontierEntry;
+constexpr int kLenBits = 24;
+constexpr int kLenMask = (1 << kLenBits) - 1;
 
+// Emits every box of the sorted slot range [first, first + count) as a hit,
+// 32 at a time (warp-collective); emitters with a faster bulk path override it.
 template <class Emit>
+__device__ __forceinline__ void emit_range_default(Emit& emit, const int* __restrict__ bid,
+                                                   long long first, long long count)
+{
+  const int lane = (int)lane_id();
+  for (long long base = 0; base < count; base += 32) {
+    const long long i = base + lane;
+    const bool hit = i < count;
+    emit(hit, hit ? __ldg(bid + first + i) : 0);
+  }
+}
+
+template <class Emit, bool kContain = true>
 __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, int K,
                                          int lane_g, int lane_c, float x1, float y1, float x2,
                                          float y2, FrontierEntry* stack, int stack_cap,
@@ -105,10 +145,16 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
     }
     return;
   }
+  // A window that contains a node's MBR hits every box under it (each box
+  // lies inside the node's MBR; a NaN box coordinate never excludes), so the
+  // subtree's slot range is emitted without descending.  A NaN in the window
+  // or the MBR fails the containment test and takes the normal path.
+  const bool contain = kContain && T.nlev > 0;
   // the root is never tested: its children range starts the frontier
   {
     int rp, rl;
     load_node_link(T, C, 0, rp, rl);
+    if (contain) rl |= max(T.nlev - 2, 0) << kLenBits;
     if (lane == 0) stack[0] = make_int2(rp, rl);
   }
   int sp = 1;
@@ -127,11 +173,14 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
       else { g = 0; c = base + lane; }
       const int gs = min(g, k - 1);
       const int pos = __shfl_sync(0xffffffffu, e.x, gs);
-      const int len = __shfl_sync(0xffffffffu, e.y, gs);
+      const int ey = __shfl_sync(0xffffffffu, e.y, gs);
+      const int len = contain ? (ey & kLenMask) : ey;
+      const int hc = contain ? (ey >> kLenBits) : 0;  // height of the nodes [pos, pos+len)
       const bool valid = g < k && c < len;
       const int child = pos + c;
-      bool hit = false, push = false;
+      bool hit = false, push = false, inside = false;
       int hid = 0, cpos = 0, clen = 0;
+      long long rfirst = 0, rcount = 0;
       if (valid) {
         if (pos >= T.rsz) {
           const int s = child - T.rsz;
@@ -145,6 +194,15 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
           load_node_box(T, C, child, a, b, cc, d);
           load_node_link(T, C, child, cpos, clen);
           push = intersects(x1, y1, x2, y2, a, b, cc, d);
+          if (contain && push && x1 <= a && cc <= x2 && y1 <= b && d <= y2) {
+            inside = true;
+            push = false;
+            const long long span = __ldg(T.lvl_span + hc);
+            rfirst = (long long)(child - __ldg(T.lvl_first + hc)) * span;
+            rcount = min((long long)T.nbox - rfirst, span);
+          } else if (contain) {
+            clen |= max(hc - 1, 0) << kLenBits;
+          }
         }
       }
       if constexpr (Emit::kCountsTests)
@@ -161,6 +219,15 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
         sp += np;
       }
       emit(hit, hid);
+      if (contain) {
+        uint32_t im = __ballot_sync(0xffffffffu, inside);
+        while (im) {
+          const int src = __ffs(im) - 1;
+          im &= im - 1;
+          emit.range(T.bid, __shfl_sync(0xffffffffu, rfirst, src),
+                     __shfl_sync(0xffffffffu, rcount, src));
+        }
+      }
     }
     __syncwarp();
   }

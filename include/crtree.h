@@ -149,9 +149,10 @@ typedef struct {
   int mode;          /* CRT_QUERY_PERSISTENT or CRT_QUERY_PLAIN */
   int sort_windows;  /* persistent: visit windows in Morton order of their centres (default 1) */
   int stage_levels;  /* persistent: stage the top tree levels in shared memory (default 1) */
-  int warps_per_cta; /* 0 = default */
+  int warps_per_cta; /* persistent: 8, 16 or 32 warps per CTA (0 = default) */
   int chunk;         /* persistent: output slots a warp reserves at a time (0 = default) */
-  int reserved[3];
+  int no_contain;    /* 1: test every box even under nodes the window contains */
+  int reserved[2];
 } crt_query_opts;
 
 void crt_query_opts_default(crt_query_opts* o);
@@ -225,8 +226,10 @@ int crt_plan_destroy(crt_plan plan);
  * arrive while others run are admitted as soon as a request slot and arena
  * memory are free, and their windows are processed alongside the others'.
  * A request is admitted by its HBM footprint: 16 bytes per window plus an
- * output estimate of 8 bytes per expected pair (running pairs-per-window
- * average of its tree times output_slack).  A request whose output outgrows
+ * output estimate of 8 bytes per expected pair (host windows: their area,
+ * clipped to the tree's root MBR, times the tree's box density and a learned
+ * correction; device windows: the tree's running pairs-per-window average;
+ * either times output_slack).  A request whose output outgrows
  * the estimate is re-run with its exact size (overflow-and-retry) before it
  * completes.  Results stay in the arena until crt_server_release. */
 typedef struct crt_server_s* crt_server;
@@ -236,7 +239,7 @@ typedef struct {
   int max_requests;        /* request slots admitted at once (default 4096) */
   int max_trees;           /* default 16 */
   double pairs_per_window; /* initial output estimate per window (default 64) */
-  double output_slack;     /* multiplier on the estimate (default 1.5, >= 1) */
+  double output_slack;     /* multiplier on the estimate (default 1.5; below 1 forces re-runs) */
   int idle_ms;             /* stop the device loop after this long without work (default 20) */
   int64_t device_wait_us;  /* bound on any device-side wait (default 2 s) */
   int reserved[4];

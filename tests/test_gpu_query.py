@@ -142,6 +142,24 @@ def test_query_nan_window_follows_tree_semantics(crt):
     assert_all(all_forms(crt, d, rt, dq), want)
 
 
+@pytest.mark.parametrize("f", [2, 3, 10, 16, 32, 40])
+def test_large_windows_containment(crt, f):
+    """Windows covering large parts of the domain: whole subtrees are emitted
+    by slot range without per-box tests; the pairs must equal the oracle's and
+    those of the box-by-box traversal (no_contain)."""
+    b = D.uniform_boxes(150_000, seed=80 + f)
+    q = D.mixed_windows(300, b, seed=180 + f, lo=0.05, hi=0.9)
+    d, rt, dq, want = setup(crt, b, q, f)
+    assert len(want[0]) > 1_000_000
+    for mode in (crt.CRT_QUERY_PERSISTENT, crt.CRT_QUERY_PLAIN):
+        for nc in (0, 1):
+            got = canon(*crt.query(rt, d, dq, mode=mode, no_contain=nc)[:2])
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (mode, nc)
+    p = crt.bfs_frontier(rt, d, dq)
+    got = canon(*p.to_host())
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
 def test_overflow_and_retry(crt):
     import torch
     b = D.uniform_boxes(100_000, seed=54)

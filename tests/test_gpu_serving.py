@@ -97,7 +97,7 @@ def test_results_same_alone_and_in_the_mix(env):
 
 def test_overflow_and_retry(env):
     C, Server, trees = env
-    srv, ids = setup_server(C, Server, trees, pairs_per_window=0.01, output_slack=1.0)
+    srv, ids = setup_server(C, Server, trees, pairs_per_window=0.01, output_slack=0.01)
     reqs = make_requests(trees, 25, seed=2)
     done = run_all(srv, ids, reqs)
     retried = sum(done[i][0]["retries"] for i in done)
