@@ -139,15 +139,21 @@ __global__ void plan_kernel(const uint32_t* __restrict__ hist, int64_t n, BuildC
 // ---------------------------------------------------------------------------
 // 3. onesweep pass
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift)
+{
+  return (k >> shift) & 0xFFu;
+}
+
+// One stable LSD pass over (key, slot) pairs for the 8-bit digit at `digit`.
+// Indices are 32-bit: the key count is below 2^31 (the C ABI's int sizes).
 __global__ void __launch_bounds__(kSortThreads, 2)
-    onesweep_kernel(int digit, SortBufs bufs, int64_t n, uint64_t* __restrict__ status,
+    onesweep_kernel(int digit, SortBufs bufs, int64_t n64, uint64_t* __restrict__ status,
                     BuildCtrl* __restrict__ ctrl)
 {
   extern __shared__ uint32_t smem[];
-  uint32_t* s_keys = smem;                       // kSortTile
-  uint32_t* s_vals = smem + kSortTile;           // kSortTile
-  uint32_t* s_whist = smem + 2 * kSortTile;      // kSortWarps * kBins
-  __shared__ int s_binstart[kBins];
+  uint32_t* s_keys = smem;                   // kSortTile
+  uint32_t* s_vals = smem + kSortTile;       // kSortTile
+  uint32_t* s_whist = smem + 2 * kSortTile;  // kSortWarps x kBins: counts, then offsets
   __shared__ int s_gbase[kBins];
   __shared__ int s_tile;
   __shared__ int s_wsum[kBins / 32];
@@ -158,81 +164,84 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   const int parity = __popc(before) & 1;
   const bool first = before == 0;
   const bool last = (active >> (digit + 1)) == 0;
-  const uint32_t* __restrict__ src_k = bufs.keys[parity];
-  const uint32_t* __restrict__ src_v = bufs.vals[parity];
-  uint32_t* __restrict__ dst_k = bufs.keys[parity ^ 1];
-  uint32_t* __restrict__ dst_v = bufs.vals[parity ^ 1];
   const int shift = digit * kRadixBits;
+  const int n = (int)n64;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(&ctrl->tile_ctr[digit], 1);
   for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) s_whist[i] = 0;
   __syncthreads();
   const int tile = s_tile;
-  const int64_t base = (int64_t)tile * kSortTile;
-  const int64_t wbase = base + (int64_t)warp * 32 * kSortIpt;
+  const int base = tile * kSortTile;
+  const int tile_n = min(kSortTile, n - base);
+  const uint32_t* __restrict__ src_k = bufs.keys[parity] + base;
+  const uint32_t* __restrict__ src_v = bufs.vals[parity] + base;
+  uint32_t* __restrict__ dst_k = bufs.keys[parity ^ 1];
+  uint32_t* __restrict__ dst_v = bufs.vals[parity ^ 1];
+  const int wbase = warp * 32 * kSortIpt + lane;  // this lane's first item in the tile
 
-  // load keys (warp-striped: item i of a lane is wbase + i*32 + lane)
+  // load keys (warp-striped: item i of a lane is wbase + 32 i)
   uint32_t key[kSortIpt];
   uint32_t rank[kSortIpt];
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
-    int64_t g = wbase + i * 32 + lane;
-    key[i] = g < n ? src_k[g] : 0u;
+    const int j = wbase + 32 * i;
+    key[i] = j < tile_n ? src_k[j] : 0u;
   }
   // rank inside the warp, stably: rounds in order, lanes in order
   uint32_t* wh = s_whist + warp * kBins;
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
-    int64_t g = wbase + i * 32 + lane;
-    uint32_t dig = g < n ? (key[i] >> shift) & 0xFF : kBins;
-    uint32_t peers = __match_any_sync(0xffffffffu, dig);
-    uint32_t old = dig < kBins ? wh[dig] : 0u;
+    const bool v = wbase + 32 * i < tile_n;
+    const uint32_t dig = v ? digit_of(key[i], shift) : kBins;
+    const uint32_t peers = __match_any_sync(0xffffffffu, dig);
+    const uint32_t old = v ? wh[dig] : 0u;
     __syncwarp();
-    if (dig < kBins && lane == (uint32_t)(__ffs(peers) - 1)) wh[dig] = old + __popc(peers);
+    if (v && (peers & lt) == 0) wh[dig] = old + __popc(peers);
     __syncwarp();
     rank[i] = old + __popc(peers & lt);
   }
   __syncthreads();
-  // per bin: exclusive over warps -> warp offsets; totals -> tile counts
+  // per bin: exclusive prefix over warps, the tile count, and the tile-local bin start
   int cnt = 0;
   if (tid < kBins) {
     int run = 0;
+#pragma unroll
     for (int w = 0; w < kSortWarps; w++) {
-      int c = (int)s_whist[w * kBins + tid];
+      const int c = (int)s_whist[w * kBins + tid];
       s_whist[w * kBins + tid] = run;
       run += c;
     }
     cnt = run;
-    // block exclusive scan of cnt over the 256 bins (8 warps)
     int x = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, x, o);
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += y;
     }
     if (lane == 31) s_wsum[warp] = x;
-    s_binstart[tid] = x - cnt;  // partial, fixed below
+    s_gbase[tid] = x - cnt;  // within this 32-bin group, completed below
   }
   __syncthreads();
   if (tid < kBins) {
-    int add = 0;
-    for (int w = 0; w < warp; w++) add += s_wsum[w];
-    s_binstart[tid] += add;
+    int binstart = s_gbase[tid];
+    for (int w = 0; w < warp; w++) binstart += s_wsum[w];
+    // fold the bin start into every warp's offset: one lookup per key later
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) s_whist[w * kBins + tid] += binstart;
 
     // decoupled look-back for bin `tid`
-    uint64_t* st = status;
     int excl = 0;
     if (tile == 0) {
-      st_relaxed_u64(&st[tid], kFlagIncl | (uint32_t)cnt);
+      st_relaxed_u64(&status[tid], kFlagIncl | (uint32_t)cnt);
     } else {
-      st_relaxed_u64(&st[(int64_t)tile * kBins + tid], kFlagAgg | (uint32_t)cnt);
+      st_relaxed_u64(&status[(int64_t)tile * kBins + tid], kFlagAgg | (uint32_t)cnt);
       int t = tile - 1;
       uint32_t spins = 0;
       while (true) {
-        uint64_t v = ld_relaxed_u64(&st[(int64_t)t * kBins + tid]);
-        uint64_t flag = v & (3ull << 62);
+        const uint64_t v = ld_relaxed_u64(&status[(int64_t)t * kBins + tid]);
+        const uint64_t flag = v & (3ull << 62);
         if (flag == 0) {
           if (++spins > kSpinLimit || ld_relaxed_i32(&ctrl->error) != 0) {
             raise_error(&ctrl->error, CRT_ERR_DEVICE_TIMEOUT);
@@ -245,29 +254,27 @@ __global__ void __launch_bounds__(kSortThreads, 2)
         if (flag == kFlagIncl) break;
         --t;
       }
-      st_relaxed_u64(&st[(int64_t)tile * kBins + tid], kFlagIncl | (uint32_t)(excl + cnt));
+      st_relaxed_u64(&status[(int64_t)tile * kBins + tid], kFlagIncl | (uint32_t)(excl + cnt));
     }
-    s_gbase[tid] = ctrl->bucket_start[digit * kBins + tid] + excl - s_binstart[tid];
+    s_gbase[tid] = ctrl->bucket_start[digit * kBins + tid] + excl - binstart;
   }
   __syncthreads();
 
-  // stage keys (and slots) in tile order of their destination
+  // stage keys and slots in the order of their destination
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
-    int64_t g = wbase + i * 32 + lane;
-    if (g < n) {
-      uint32_t dig = (key[i] >> shift) & 0xFF;
-      int pos = s_binstart[dig] + (int)s_whist[warp * kBins + dig] + (int)rank[i];
+    const int j = wbase + 32 * i;
+    if (j < tile_n) {
+      const int pos = (int)(wh[digit_of(key[i], shift)] + rank[i]);
       s_keys[pos] = key[i];
-      s_vals[pos] = first ? (uint32_t)g : src_v[g];
+      s_vals[pos] = first ? (uint32_t)(base + j) : src_v[j];
     }
   }
   __syncthreads();
-  const int tile_n = (int)min((int64_t)kSortTile, n - base);
   for (int j = tid; j < tile_n; j += kSortThreads) {
-    uint32_t k = s_keys[j];
-    int dst = s_gbase[(k >> shift) & 0xFF] + j;
-    if ((uint32_t)dst < (uint64_t)n) {
+    const uint32_t k = s_keys[j];
+    const int dst = s_gbase[digit_of(k, shift)] + j;
+    if ((uint32_t)dst < (uint32_t)n) {
       if (!last) dst_k[dst] = k;
       dst_v[dst] = s_vals[j];
     }
@@ -319,23 +326,39 @@ __global__ void __launch_bounds__(kLevelThreads)
   bool init = false;
   for (int64_t cb = c0; cb < c1; cb += kLevelChunk) {
     const int64_t ce = min(c1, cb + (int64_t)kLevelChunk);
-    for (int64_t s = cb + threadIdx.x; s < ce; s += kLevelThreads) {
-      float4 m;
-      if (kLeaf) {
-        int64_t src = sorted ? (int64_t)sorted[s] : s;
-        if (src >= nchild) src = s;  // only reachable after a sort error (reported)
-        Box32 bx = aos[src];
-        m = bx.mbr;
-        oxmin[s] = m.x;
-        oymin[s] = m.y;
-        oxmax[s] = m.z;
-        oymax[s] = m.w;
-        oid[s] = bx.idp.x;
-      } else {
-        const int64_t i = child_start + s;
-        m = make_float4(nxmin[i], nymin[i], nxmax[i], nymax[i]);
+    if (kLeaf) {
+      // all slot loads, then all 32-byte record loads, then the stores: each
+      // thread keeps kGather random sector reads in flight
+      constexpr int kGather = kLevelChunk / kLevelThreads;
+      int64_t src[kGather];
+#pragma unroll
+      for (int u = 0; u < kGather; u++) {
+        const int64_t s = cb + threadIdx.x + u * kLevelThreads;
+        src[u] = s < ce ? (sorted ? (int64_t)sorted[s] : s) : 0;
+        if (src[u] >= nchild) src[u] = s < ce ? s : 0;  // only after a sort error (reported)
       }
-      s_mbr[s - cb] = m;
+      Box32 bx[kGather];
+#pragma unroll
+      for (int u = 0; u < kGather; u++)
+        if (cb + threadIdx.x + u * kLevelThreads < ce) bx[u] = aos[src[u]];
+#pragma unroll
+      for (int u = 0; u < kGather; u++) {
+        const int64_t s = cb + threadIdx.x + u * kLevelThreads;
+        if (s < ce) {
+          const float4 m = bx[u].mbr;
+          oxmin[s] = m.x;
+          oymin[s] = m.y;
+          oxmax[s] = m.z;
+          oymax[s] = m.w;
+          oid[s] = bx[u].idp.x;
+          s_mbr[s - cb] = m;
+        }
+      }
+    } else {
+      for (int64_t s = cb + threadIdx.x; s < ce; s += kLevelThreads) {
+        const int64_t i = child_start + s;
+        s_mbr[s - cb] = make_float4(nxmin[i], nymin[i], nxmax[i], nymax[i]);
+      }
     }
     __syncthreads();
     if (have) {

@@ -111,9 +111,9 @@ def test_overflow_and_retry(env):
 
 def test_admission_by_footprint(env):
     C, Server, trees = env
-    # room for about one request of this size at a time
-    srv, ids = setup_server(C, Server, trees, arena_bytes=4 << 20, pairs_per_window=50.0)
-    w = D.mixed_windows(4000, trees[0]["sb"], seed=77, lo=1e-5, hi=1e-3)
+    # the windows alone (16 B each, 2.4 MB) leave room for one request at a time
+    srv, ids = setup_server(C, Server, trees, arena_bytes=4 << 20, pairs_per_window=1.0)
+    w = D.mixed_windows(150_000, trees[0]["sb"], seed=77, lo=1e-5, hi=1e-4)
     a = srv.submit(ids[0], w)
     assert a is not None
     b = srv.submit(ids[0], w)
