@@ -120,6 +120,10 @@ SIGNATURES = {
                                        ctypes.POINTER(crt_bbox_f32), _i64, _vp, _vp, _i64, _vp,
                                        ctypes.POINTER(crt_query_opts), _vp,
                                        ctypes.POINTER(_vp)]),
+    "crt_query_plain_noalloc_f32": (ctypes.c_int, [ctypes.POINTER(crt_rtree_f32),
+                                                   ctypes.POINTER(crt_bbox_f32),
+                                                   ctypes.POINTER(crt_bbox_f32), _vp, _vp, _i64,
+                                                   _vp, _vp]),
     "crt_query_stats_f32": (ctypes.c_int, [ctypes.POINTER(crt_rtree_f32),
                                            ctypes.POINTER(crt_bbox_f32),
                                            ctypes.POINTER(crt_bbox_f32), _vp, _vp,

@@ -55,6 +55,9 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
 int plan_set_nq(void* p, int64_t nq, cudaStream_t stream);
 int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
                 int64_t* d_hits, int64_t* d_tested, int64_t* h_totals, cudaStream_t stream);
+int query_plain_noalloc(const crt_rtree_f32& rt, const crt_bbox_f32& rbox,
+                        const crt_bbox_f32& qbox, int32_t* fid, int32_t* tid, int64_t capacity,
+                        crt_query_result* d_result, cudaStream_t stream);
 int plan_launch(void* p, cudaStream_t stream);
 int plan_destroy(void* p);
 
@@ -323,6 +326,16 @@ int crt_query_sync_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   if (h.error) return fail(h.error, "query_sync: device-side error");
   if (h.overflow) return fail(CRT_ERR_OUTPUT_OVERFLOW, "query_sync: output too small");
   return CRT_OK;
+}
+
+int crt_query_plain_noalloc_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                                const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
+                                int64_t capacity, crt_query_result* d_result, crt_stream_t stream)
+{
+  if (!tree_ok(d_rt) || !box_ok(d_rbox) || !box_ok(d_qbox))
+    return fail(CRT_ERR_INVALID_ARG, "query_plain_noalloc: bad arguments");
+  return query_plain_noalloc(*d_rt, *d_rbox, *d_qbox, d_fid, d_tid, capacity, d_result,
+                             (cudaStream_t)stream);
 }
 
 int crt_query_stats_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,

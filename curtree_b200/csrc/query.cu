@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "internal.h"
@@ -942,6 +943,106 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "query (persistent)");
   (void)sms;
+  return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plain query without allocation
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory while they run: a process whose
+// device memory is owned by another allocator (an engine that reserves the
+// GPU's memory up front and must account for every byte), or a
+// latency-critical loop that cannot afford cudaMalloc's implicit device
+// synchronisation.  For them the plain query has a variant whose scratch --
+// counters, per-window counts, scan partials, offsets and containment tables
+// -- lives in this fixed device array instead of the stream-ordered pool.
+//
+// The array is a module global: every GPU that loads the library holds its
+// 1 MiB until the process exits.  In host code `g_noalloc_scratch` is only a
+// host-side stand-in; the device address comes from cudaGetSymbolAddress,
+// looked up once per device (the first call on a device does it, with that
+// device current).  All calls share the array and it keeps the last call's
+// contents, so the counters are cleared on every call; calls whose work
+// overlaps on the GPU (different streams, or another thread) race on it and
+// must be serialised by the caller.
+constexpr int64_t kNoAllocMaxWindows = 1 << 16;
+constexpr size_t kNoAllocCountsOff = 256;
+constexpr size_t kNoAllocSumsOff = kNoAllocCountsOff + 8 * (size_t)kNoAllocMaxWindows;
+constexpr size_t kNoAllocOffsetsOff = kNoAllocSumsOff + 8 * 256;
+constexpr size_t kNoAllocTablesOff =
+    (kNoAllocOffsetsOff + 8 * (size_t)(kNoAllocMaxWindows + 1) + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes = kNoAllocTablesOff + (kLevelTableBytes + 255) / 256 * 256;
+static_assert(kNoAllocBytes <= (1u << 20) + 4096, "no-alloc scratch stays near 1 MiB");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+static int noalloc_scratch_address(char** out)
+{
+  static std::mutex mu;
+  static std::vector<std::pair<int, char*>> addr;  // device -> device address of the array
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "query_plain_noalloc: cudaGetDevice");
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& a : addr)
+    if (a.first == dev) {
+      *out = a.second;
+      return CRT_OK;
+    }
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "query_plain_noalloc: cudaGetSymbolAddress");
+  addr.emplace_back(dev, (char*)p);
+  *out = (char*)p;
+  return CRT_OK;
+}
+
+int query_plain_noalloc(const crt_rtree_f32& rt, const crt_bbox_f32& rbox,
+                        const crt_bbox_f32& qbox, int32_t* fid, int32_t* tid, int64_t capacity,
+                        crt_query_result* d_result, cudaStream_t stream)
+{
+  if (!d_result) return fail(CRT_ERR_INVALID_ARG, "query_plain_noalloc: result block is required");
+  if (qbox.sz < 0 || rbox.sz < 0 || rt.sz < 0 || capacity < 0)
+    return fail(CRT_ERR_INVALID_ARG, "query_plain_noalloc: negative size");
+  if (qbox.sz > kNoAllocMaxWindows)
+    return fail(CRT_ERR_INVALID_ARG,
+                "query_plain_noalloc: at most 65536 windows per call (fixed scratch); "
+                "split the batch or use crt_query_into_f32");
+  if (rt.sz > 0 && rt.fanout < 2) return fail(CRT_ERR_INVALID_ARG, "query_plain_noalloc: fanout < 2");
+  if (capacity > 0 && (!fid || !tid))
+    return fail(CRT_ERR_INVALID_ARG, "query_plain_noalloc: null output");
+  char* scr = nullptr;
+  int rc = noalloc_scratch_address(&scr);
+  if (rc != CRT_OK) return rc;
+  TreeView T = make_view(rt, rbox);
+  attach_levels(T, level_tables(rt, rbox.sz), scr + kNoAllocTablesOff, stream);
+  WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};
+  const int64_t nq = qbox.sz;
+  const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
+  QueryCounters* ctr = (QueryCounters*)scr;
+  long long* counts = (long long*)(scr + kNoAllocCountsOff);
+  long long* sums = (long long*)(scr + kNoAllocSumsOff);
+  long long* offsets = (long long*)(scr + kNoAllocOffsetsOff);
+  const int64_t nb = std::max<int64_t>(1, cdiv(nq, kScanThreads));
+  cudaMemsetAsync(ctr, 0, sizeof(QueryCounters), stream);
+  cudaMemsetAsync(offsets, 0, 8, stream);
+  const size_t smem = (size_t)kPlainWarps * sh.stack_cap * sizeof(FrontierEntry);
+  cudaFuncSetAttribute(plain_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(plain_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (nq > 0) {
+    const unsigned g = (unsigned)cdiv(nq, kPlainWarps);
+    plain_count_kernel<<<g, kPlainWarps * 32, smem, stream>>>(T, W, sh.K, sh.stack_cap, counts, ctr);
+    scan_block_sums<<<(unsigned)nb, kScanThreads, 0, stream>>>(counts, nq, sums);
+    scan_sums_kernel<<<1, kScanThreads, 0, stream>>>(sums, nb);
+    scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, stream>>>(counts, nq, sums, offsets);
+    plain_write_kernel<<<g, kPlainWarps * 32, smem, stream>>>(T, W, sh.K, sh.stack_cap, offsets,
+                                                              fid, tid, capacity, ctr);
+    CRT_LAUNCHED(5);
+  }
+  plain_result_kernel<<<1, 1, 0, stream>>>(offsets, nq, capacity, ctr, d_result);
+  CRT_LAUNCHED(1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "query_plain_noalloc");
   return CRT_OK;
 }
 

@@ -193,6 +193,22 @@ int crt_query_sync_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                        int64_t capacity, int64_t* count, int64_t* required,
                        const crt_query_opts* opts, crt_stream_t stream);
 
+/* The plain query (CRT_QUERY_PLAIN of crt_query_into_f32: the same pairs in
+ * the same order, grouped by window) for callers that cannot allocate device
+ * memory while they run -- a process whose device memory belongs to another
+ * allocator or budget, or a loop that cannot take cudaMalloc's implicit
+ * synchronisation.  No counterpart in the reference.  It allocates nothing:
+ * its scratch is a fixed 1 MiB device array inside the library (held by every
+ * GPU that loads the library until exit), so a call takes at most 65536
+ * windows (more gives CRT_ERR_INVALID_ARG).  The caller passes the tree, the
+ * windows, the output arrays and the device result block as usual.  The first
+ * call on a device looks up the array's device address (with that device
+ * current).  Calls share the array: calls whose work overlaps on the GPU
+ * race, so serialise them (one stream, one thread at a time). */
+int crt_query_plain_noalloc_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
+                                const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
+                                int64_t capacity, crt_query_result* d_result, crt_stream_t stream);
+
 /* Per-window workload statistics: hit count and number of leaf boxes tested
  * (int64 device arrays of nq entries, either may be NULL); totals[0] = all
  * hits, totals[1] = all leaf boxes tested (host, may be NULL).  Synchronous.
