@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--warps", type=int, default=0, help="warps per CTA of the persistent traversal")
     p.add_argument("--stage", type=int, default=1, help="stage the top tree levels in shared memory")
     p.add_argument("--sort-windows", type=int, default=1)
+    p.add_argument("--autotune", type=int, default=1, help="pick fanout/warps/staging first (untimed)")
+    p.add_argument("--autotune-windows", type=int, default=100_000)
     p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu,serve")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
     p.add_argument("--serve-requests", type=int, default=300)
@@ -175,6 +177,17 @@ def make_query_inputs(rank: int, nbox: int, nwin: int):
     return boxes, windows
 
 
+def reduce_max(x: float, dist, device="cuda") -> float:
+    """Max of a per-rank value over all ranks (the step time the JSON line
+    reports); the identity on one process."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def timed(fn, steps, stream):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -215,6 +228,21 @@ def run_ours(args, rank, world, dist):
     # ---- inputs resident in HBM -------------------------------------------
     boxes, windows = make_query_inputs(rank, args.boxes, args.windows)
     d_in = C.BBox.from_host(boxes)
+    tuned = None
+    if args.autotune:
+        # untimed: pick fanout / warps / staging on a sample of the windows
+        from curtree_b200.autotune import autotune
+        sample = windows.take(np.arange(0, windows.n, max(1, windows.n // args.autotune_windows)))
+        tuned = autotune(d_in, C.BBox.from_host(sample), cache_path=None, reps=2)
+        args.fanout = tuned["fanout"]
+        args.warps = tuned["warps_per_cta"]
+        args.stage = tuned["stage_levels"]
+        torch.cuda.empty_cache()
+    out["autotune"] = None if tuned is None else {
+        "chosen": {k: tuned[k] for k in ("fanout", "warps_per_cta", "stage_levels", "chunk", "ms")},
+        "sample_windows": int(sample.n),
+        "table": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in row.items()}
+                  for row in tuned["table"]]}
     sorted_box, rt = C.build_into(d_in, args.fanout)
     del d_in
     d_win = C.BBox.from_host(windows)
@@ -246,11 +274,7 @@ def run_ours(args, rank, world, dist):
     profile_collect(None)
     r = C.read_result(res)
     assert r["overflow"] == 0 and r["count"] == pairs, r
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = reduce_max(ms, dist)
     step_ms = ms_max / args.steps
     kern_ms = k_ms / max(k_n, 1) if k_n else step_ms
     alg_bytes = 16 * args.windows + 16 * tested + 12 * pairs
@@ -283,10 +307,7 @@ def run_ours(args, rank, world, dist):
         pms = timed(plain, args.steps, stream)
         pk_ms, pk_n = profile_collect("traverse_plain")
         profile_collect(None)
-        if dist is not None:
-            t = torch.tensor([pms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
+        pms = reduce_max(pms, dist)
         out["plain"] = {"ms_per_step": pms / args.steps,
                         "windows_per_s": world * args.windows / (pms / args.steps / 1e3),
                         "kernel_ms": pk_ms / max(args.steps, 1)}
@@ -345,10 +366,7 @@ def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, d
     r = C.read_result(h_res)
     assert r["count"] == pairs and r["overflow"] == 0, r
     ms = timed(step, args.steps, stream)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist)
     h2d = sum(int(h.numel() * h.element_size()) for h in h_win)
     return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * pairs + 64,
@@ -501,10 +519,7 @@ def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
     parts = {k: profile_collect(k)[0] / args.steps for k in ("encode", "sort_pass", "level")}
     profile_collect(None)
     L.crt_profile_enable(0)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist)
     kern_ms = sum(parts.values())
     b_build = 120 * n + 40 * rsz
     strict = 40 * n + 24 * rsz
@@ -579,7 +594,7 @@ def main():
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
                 "plain": out.get("plain"), "build": out.get("build"),
                 "serving": out.get("serving"),
-                "workload_stats": out["workload_stats"],
+                "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                 "persistent_kernel_ms": p["kernel_ms"]}
         if "plain" in out:
             line["persistent_vs_plain"] = p["windows_per_s"] / out["plain"]["windows_per_s"]

@@ -111,6 +111,14 @@ SIGNATURES = {
                                           ctypes.POINTER(crt_bbox_f32), _vp, _vp, _i64, _vp, _vp,
                                           ctypes.POINTER(crt_query_opts), _vp]),
     "crt_query_capacity": (_i64, [_i64, ctypes.POINTER(crt_query_opts)]),
+    "crt_pairs_canonicalize": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "crt_read_mbr_csv": (ctypes.c_int, [ctypes.c_char_p, _i64, ctypes.c_float, _vp, _vp, _vp, _vp,
+                                        _vp, ctypes.POINTER(_i64)]),
+    "crt_tree_save": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(crt_rtree_f32),
+                                     ctypes.POINTER(crt_bbox_f32)]),
+    "crt_tree_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(crt_rtree_f32),
+                                     ctypes.POINTER(crt_bbox_f32)]),
+    "crt_bbox_free": (ctypes.c_int, [ctypes.POINTER(crt_bbox_f32)]),
     "crt_query_sync_f32": (ctypes.c_int, [ctypes.POINTER(crt_rtree_f32),
                                           ctypes.POINTER(crt_bbox_f32),
                                           ctypes.POINTER(crt_bbox_f32), _vp, _vp, _i64,

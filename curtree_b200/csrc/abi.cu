@@ -328,6 +328,12 @@ int crt_query_sync_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   return CRT_OK;
 }
 
+int crt_pairs_canonicalize(int32_t* d_fid, int32_t* d_tid, int64_t n, crt_stream_t stream)
+{
+  init_device();
+  return pairs_canonicalize(d_fid, d_tid, n, (cudaStream_t)stream);
+}
+
 int crt_query_plain_noalloc_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                                 const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
                                 int64_t capacity, crt_query_result* d_result, crt_stream_t stream)

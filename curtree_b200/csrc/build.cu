@@ -163,7 +163,7 @@ __device__ __forceinline__ uint32_t peer_mask(uint32_t v)
 // Indices are 32-bit: the key count is below 2^31 (the C ABI's int sizes).
 __global__ void __launch_bounds__(kSortThreads, 2)
     onesweep_kernel(int digit, SortBufs bufs, int64_t n64, uint64_t* __restrict__ status,
-                    BuildCtrl* __restrict__ ctrl)
+                    BuildCtrl* __restrict__ ctrl, int flags)
 {
   extern __shared__ uint32_t smem[];
   uint32_t* s_keys = smem;                   // kSortTile
@@ -177,8 +177,8 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   if (!((active >> digit) & 1)) return;
   const int before = active & ((1 << digit) - 1);
   const int parity = __popc(before) & 1;
-  const bool first = before == 0;
-  const bool last = (active >> (digit + 1)) == 0;
+  const bool first = before == 0 && !(flags & kSortGivenValues);
+  const bool last = (active >> (digit + 1)) == 0 && !(flags & kSortKeepKeys);
   const int shift = digit * kRadixBits;
   const int n = (int)n64;
 
@@ -435,7 +435,7 @@ static uint64_t* sort_status(void* zero_block)
   return (uint64_t*)((char*)zero_block + sizeof(SortCtrl) + 4 * kBins * sizeof(uint32_t));
 }
 
-void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream)
+void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream, int flags)
 {
   const int64_t ntiles = sort_tiles(n);
   SortCtrl* ctrl = sort_ctrl(zero_block);
@@ -446,7 +446,7 @@ void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream
   for (int d = 0; d < 4; d++) {
     ProfScope ps("sort_pass", stream);
     onesweep_kernel<<<(unsigned)ntiles, kSortThreads, smem, stream>>>(
-        d, bufs, n, status + (size_t)d * ntiles * kBins, ctrl);
+        d, bufs, n, status + (size_t)d * ntiles * kBins, ctrl, flags);
   }
   CRT_LAUNCHED(5);
 }

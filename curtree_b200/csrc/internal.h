@@ -35,7 +35,12 @@ size_t sort_zero_bytes(int64_t n);
 // Enqueues plan + four onesweep passes; keys must be in bufs.keys[0] and the
 // histograms filled.  The sorted positions end in bufs.vals[n_active & 1]
 // (identity when no pass is active).
-void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream);
+// flags: kSortGivenValues -- the values are in bufs.vals[0] (otherwise the
+// first pass makes them: positions 0..n-1); kSortKeepKeys -- the sorted keys
+// are kept too, in bufs.keys[n_active & 1] (otherwise the last pass drops them).
+constexpr int kSortGivenValues = 1;
+constexpr int kSortKeepKeys = 2;
+void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream, int flags = 0);
 uint32_t* sort_hist(void* zero_block);
 SortCtrl* sort_ctrl(void* zero_block);
 
@@ -46,6 +51,8 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
                float* out_ymin, float* out_xmax, float* out_ymax, int* out_id, float* nxmin,
                float* nymin, float* nxmax, float* nymax, int* npos, int* nlen,
                cudaStream_t stream);
+
+int pairs_canonicalize(int32_t* fid, int32_t* tid, int64_t n, cudaStream_t stream);
 
 // Query entry used by the C ABI.
 int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,

@@ -213,6 +213,14 @@ def bfs_thrust(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, stream=None) -> IDPair:
     return _query_dropin(load().crt_query_thrust_f32, "bfs_thrust", d_rt, d_rbox, d_qbox, stream)
 
 
+def canonicalize(fid, tid, stream=None) -> None:
+    """Sort pair tensors in place into (window, box id) order on the GPU."""
+    n = int(fid.numel())
+    check(load().crt_pairs_canonicalize(fid.data_ptr() if n else None,
+                                        tid.data_ptr() if n else None, n,
+                                        _stream_handle(stream)), "canonicalize")
+
+
 def query_capacity(pairs: int, mode: int = _lib.CRT_QUERY_PERSISTENT) -> int:
     o = _lib.default_opts(mode=mode)
     return int(load().crt_query_capacity(pairs, ctypes.byref(o)))

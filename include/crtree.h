@@ -181,6 +181,12 @@ int crt_query_into_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                        int64_t capacity, crt_query_result* d_result, int64_t* d_offsets,
                        const crt_query_opts* opts, crt_stream_t stream);
 
+/* Sorts n pairs in place into (window, box id) order, both ascending as
+ * signed ints: the order the reference's drivers produce with two host
+ * stable sorts (src/rtree_test_frontier.cu:102-105), here on the GPU.
+ * Synchronous; at most INT32_MAX pairs per call. */
+int crt_pairs_canonicalize(int32_t* d_fid, int32_t* d_tid, int64_t n, crt_stream_t stream);
+
 /* Output slots to allocate for `pairs` hit pairs so that a PERSISTENT query
  * cannot overflow (adds the per-warp reservation slack). */
 int64_t crt_query_capacity(int64_t pairs, const crt_query_opts* opts);
@@ -231,6 +237,29 @@ int crt_plan_create(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
 int crt_plan_set_nq(crt_plan plan, int64_t nq, crt_stream_t stream);
 int crt_plan_launch(crt_plan plan, crt_stream_t stream);
 int crt_plan_destroy(crt_plan plan);
+
+/* ---------------------------------------------------------------------- */
+/* Ingest and persistence                                                   */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces readMBR (src/utility.cpp:5-40): reads n records
+ * "x1,y1,x2,y2,id,pid,nume" from a text file into HOST arrays as the boxes
+ * [min(x1,x2) - r, max(x1,x2) + r] x [min(y1,y2) - r, max(y1,y2) + r] with
+ * their ids (fp32 arithmetic and %f/%d parsing as the reference's fscanf).
+ * A missing file, a malformed record or fewer than n records give
+ * CRT_ERR_INVALID_ARG (the reference exits or throws); *n_read = records
+ * parsed before the problem. */
+int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* ymin, float* xmax,
+                     float* ymax, int32_t* id, int64_t* n_read);
+
+/* Writes a built tree and its sorted box set to a file (no reference
+ * counterpart; format in curtree_b200/csrc/io.cu). */
+int crt_tree_save(const char* path, const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox);
+/* Reads such a file into newly cudaMalloc'd device arrays (free with
+ * crt_rtree_free and crt_bbox_free); the result can be queried at once. */
+int crt_tree_load(const char* path, crt_rtree_f32* d_rt, crt_bbox_f32* d_rbox);
+/* Replaces box_d_free (src/utility.cuh:68-89): cudaFree the five arrays. */
+int crt_bbox_free(crt_bbox_f32* d_box);
 
 /* ---------------------------------------------------------------------- */
 /* Serving loop (no reference counterpart: the reference answers one batch   */

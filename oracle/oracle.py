@@ -88,6 +88,8 @@ def ref_cpu():
         R.ref_nested_loop_query.argtypes = args + [_i32p, _i32p, _i64]
         R.ref_nested_loop_query_mt.restype = _i64
         R.ref_nested_loop_query_mt.argtypes = args + [ctypes.c_int]
+        R.ref_read_mbr.restype = ctypes.c_int
+        R.ref_read_mbr.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_float] + [_f32p] * 4 + [_i32p]
         _ref = R
     return _ref
 
@@ -255,6 +257,16 @@ def ref_nested_loop_pairs(q, d, positional_qid: bool = True) -> tuple[np.ndarray
     qo = np.empty(max(n, 1), np.int32)
     R.ref_nested_loop_query(*args, did, qo, n)
     return did[:n], qo[:n]
+
+
+def ref_read_mbr(path: str, n: int, r: float):
+    """The reference's own readMBR (src/utility.cpp:5-40) on an existing file."""
+    from curtree_b200.datasets import HostBoxes
+    out = HostBoxes(*(np.empty(n, np.float32) for _ in range(4)), np.empty(n, np.int32))
+    rc = ref_cpu().ref_read_mbr(path.encode(), n, r, out.xmin, out.ymin, out.xmax, out.ymax, out.id)
+    if rc != 0:
+        raise ValueError("reference readMBR rejected the file")
+    return out
 
 
 def canonical_pairs(fid: np.ndarray, tid: np.ndarray) -> tuple[np.ndarray, np.ndarray]:

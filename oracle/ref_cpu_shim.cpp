@@ -84,3 +84,27 @@ extern "C" int64_t ref_nested_loop_query_mt(const float* qxmin, const float* qym
   for (auto c : counts) total += c;
   return total;
 }
+
+// The reference's readMBR (src/utility.cpp:5-40), compiled from its source,
+// copied out into caller arrays.  Returns 0, or -1 when it throws (it exits on
+// a missing file, so callers pass existing files only).
+extern "C" int ref_read_mbr(const char* path, int size, float r, float* xmin, float* ymin,
+                            float* xmax, float* ymax, int* id)
+{
+  float *a = nullptr, *b = nullptr, *c = nullptr, *d = nullptr;
+  int* e = nullptr;
+  try {
+    readMBR(const_cast<char*>(path), size, r, a, b, c, d, e);
+  } catch (const std::exception&) {
+    return -1;
+  }
+  for (int i = 0; i < size; i++) {
+    xmin[i] = a[i];
+    ymin[i] = b[i];
+    xmax[i] = c[i];
+    ymax[i] = d[i];
+    id[i] = e[i];
+  }
+  delete[] a; delete[] b; delete[] c; delete[] d; delete[] e;
+  return 0;
+}

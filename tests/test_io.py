@@ -1,0 +1,90 @@
+"""Ingest without a GPU: crt_read_mbr_csv (host code in the library) against
+the reference's own readMBR compiled from src/utility.cpp -- bit-identical
+boxes and ids -- and its error statuses where the reference exits or throws."""
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from curtree_b200 import _lib
+from oracle import oracle as O
+
+
+def write_csv(path, rows, fmt):
+    with open(path, "w") as f:
+        for r in rows:
+            f.write(fmt(r) + "\n")
+
+
+def read_ours(path, n, r):
+    L = _lib.load()
+    a = [np.empty(n, np.float32) for _ in range(4)]
+    ids = np.empty(n, np.int32)
+    got = ctypes.c_int64(0)
+    st = L.crt_read_mbr_csv(path.encode(), n, r, *[x.ctypes.data for x in a], ids.ctypes.data,
+                            ctypes.byref(got))
+    return st, got.value, a, ids
+
+
+def make_rows(n, seed):
+    rng = np.random.default_rng(seed)
+    x1 = rng.uniform(-1e5, 1e5, n)
+    y1 = rng.uniform(-1e5, 1e5, n)
+    x2 = x1 + rng.normal(0, 50, n)
+    y2 = y1 + rng.normal(0, 50, n)
+    ids = rng.integers(-2**31, 2**31 - 1, n)
+    return list(zip(x1, y1, x2, y2, ids, rng.integers(0, 100, n), rng.integers(0, 9, n)))
+
+
+FORMATS = {
+    "plain": lambda r: f"{r[0]:.6f},{r[1]:.6f},{r[2]:.6f},{r[3]:.6f},{r[4]},{r[5]},{r[6]}",
+    "long": lambda r: f"{float(r[0])!r},{float(r[1])!r},{float(r[2])!r},{float(r[3])!r},{r[4]},{r[5]},{r[6]}",
+    "sci": lambda r: f"{r[0]:.9e},{r[1]:.3e},{r[2]:.12e},{r[3]:g},{r[4]},{r[5]},{r[6]}",
+    "spaced": lambda r: f" {r[0]:.4f}, {r[1]:.4f},\t{r[2]:.4f},{r[3]:.4f}, {r[4]},{r[5]},{r[6]}  ",
+}
+
+
+@pytest.mark.skipif(not O.ref_cpu_available(), reason="reference CPU build absent")
+@pytest.mark.parametrize("fmt", sorted(FORMATS))
+@pytest.mark.parametrize("r", [0.0, 10.0, 0.37])
+def test_read_mbr_matches_reference(fmt, r):
+    rows = make_rows(5000, seed=hash(fmt) % 1000)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "mbr.csv")
+        write_csv(path, rows, FORMATS[fmt])
+        ref = O.ref_read_mbr(path, len(rows), r)
+        st, got, a, ids = read_ours(path, len(rows), r)
+        assert st == _lib.CRT_OK and got == len(rows)
+        for mine, theirs in zip(a, (ref.xmin, ref.ymin, ref.xmax, ref.ymax)):
+            assert np.array_equal(mine.view(np.uint32), theirs.view(np.uint32))
+        assert np.array_equal(ids, ref.id)
+
+
+@pytest.mark.skipif(not O.ref_cpu_available(), reason="reference CPU build absent")
+def test_blank_before_separator_rejected_like_reference():
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "b.csv")
+        with open(path, "w") as f:
+            f.write("1,2,3,4,5,6,7\n1,2,3 ,4,5,6,7\n")
+        with pytest.raises(ValueError):
+            O.ref_read_mbr(path, 2, 0.0)
+        st, got, _, _ = read_ours(path, 2, 0.0)
+        assert st == _lib.CRT_ERR_INVALID_ARG and got == 1
+
+
+def test_read_mbr_errors():
+    with tempfile.TemporaryDirectory() as tmp:
+        st, got, _, _ = read_ours(os.path.join(tmp, "missing.csv"), 10, 0.0)
+        assert st == _lib.CRT_ERR_INVALID_ARG
+        path = os.path.join(tmp, "short.csv")
+        write_csv(path, make_rows(7, 1), FORMATS["plain"])
+        st, got, _, _ = read_ours(path, 10, 0.0)
+        assert st == _lib.CRT_ERR_INVALID_ARG and got == 7
+        path = os.path.join(tmp, "bad.csv")
+        with open(path, "w") as f:
+            f.write("1,2,3,4,5,6,7\n1,2,x,4,5,6,7\n1,2,3,4,5,6,7\n")
+        st, got, _, _ = read_ours(path, 3, 0.0)
+        assert st == _lib.CRT_ERR_INVALID_ARG and got == 1
+        assert b"record 1" in _lib.load().crt_last_error()
