@@ -74,8 +74,13 @@ struct StatEmit {
   long long tested = 0;
   __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
+  long long range_hits = 0;
   __device__ __forceinline__ void leaf_tests(int n) { tested += n; }
-  __device__ __forceinline__ void range(const int*, long long, long long count) { hits += count; }
+  __device__ __forceinline__ void range(const int*, long long, long long count)
+  {
+    hits += count;
+    range_hits += count;
+  }
 };
 
 // Writes at precomputed per-window offsets (plain write pass).
@@ -211,6 +216,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
            s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
 }
 
+template <bool kContain>
 __global__ void __launch_bounds__(kPlainWarps * 32)
     stats_kernel(TreeView T, WindowView W, int K, int stack_cap, long long* __restrict__ hits,
                  long long* __restrict__ tested, unsigned long long* __restrict__ totals,
@@ -224,13 +230,14 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
   lane_map(T.fanout, K, lg, lc);
   NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   StatEmit emit;
-  traverse<StatEmit, false>(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
-                            s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
+  traverse<StatEmit, kContain>(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
+                               s_stack + warp * stack_cap, stack_cap, emit, &ctr->error);
   if (lane_id() == 0) {
     if (hits) hits[q] = emit.hits;
     if (tested) tested[q] = emit.tested;
     atomicAdd(&totals[0], (unsigned long long)emit.hits);
     atomicAdd(&totals[1], (unsigned long long)emit.tested);
+    atomicAdd(&totals[2], (unsigned long long)emit.range_hits);
   }
 }
 
@@ -1049,25 +1056,33 @@ int query_plain_noalloc(const crt_rtree_f32& rt, const crt_bbox_f32& rbox,
 int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
                 int64_t* d_hits, int64_t* d_tested, int64_t* h_totals, cudaStream_t stream)
 {
-  const TreeView T = make_view(rt, rbox);
+  TreeView T = make_view(rt, rbox);
   WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};
   const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
   char* scr = nullptr;
-  if (cudaMallocAsync((void**)&scr, 512, stream) != cudaSuccess) {
+  if (cudaMallocAsync((void**)&scr, 1024 + kLevelTableBytes, stream) != cudaSuccess) {
     cudaGetLastError();
     return fail(CRT_ERR_OOM, "query_stats: scratch allocation failed");
   }
   QueryCounters* ctr = (QueryCounters*)scr;
-  unsigned long long* tot = (unsigned long long*)(scr + 256);
-  cudaMemsetAsync(scr, 0, 512, stream);
+  unsigned long long* tot = (unsigned long long*)(scr + 256);  // [3] box-by-box, [3] containment
+  cudaMemsetAsync(scr, 0, 1024, stream);
   const size_t smem = (size_t)kPlainWarps * sh.stack_cap * sizeof(FrontierEntry);
-  cudaFuncSetAttribute(stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(stats_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(stats_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (qbox.sz > 0) {
-    stats_kernel<<<(unsigned)cdiv(qbox.sz, kPlainWarps), kPlainWarps * 32, smem, stream>>>(
+    const unsigned g = (unsigned)cdiv(qbox.sz, kPlainWarps);
+    // the reference algorithm: every leaf box under an intersecting node is tested
+    stats_kernel<false><<<g, kPlainWarps * 32, smem, stream>>>(
         T, W, sh.K, sh.stack_cap, (long long*)d_hits, (long long*)d_tested, tot, ctr);
-    CRT_LAUNCHED(1);
+    // this library's: contained subtrees are emitted by slot range
+    TreeView Tc = T;
+    attach_levels(Tc, level_tables(rt, rbox.sz), scr + 1024, stream);
+    stats_kernel<true><<<g, kPlainWarps * 32, smem, stream>>>(Tc, W, sh.K, sh.stack_cap, nullptr,
+                                                              nullptr, tot + 3, ctr);
+    CRT_LAUNCHED(2);
   }
-  unsigned long long h[2] = {0, 0};
+  unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
   int err = 0;
   cudaMemcpyAsync(h, tot, sizeof(h), cudaMemcpyDeviceToHost, stream);
   cudaMemcpyAsync(&err, &ctr->error, sizeof(int), cudaMemcpyDeviceToHost, stream);
@@ -1075,9 +1090,12 @@ int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "query_stats");
   if (err) return fail(err, "query_stats: device-side error");
+  if (h[0] != h[3]) return fail(CRT_ERR_CUDA, "query_stats: the two traversals disagree on the pair count");
   if (h_totals) {
-    h_totals[0] = (int64_t)h[0];
-    h_totals[1] = (int64_t)h[1];
+    h_totals[0] = (int64_t)h[0];  // hits
+    h_totals[1] = (int64_t)h[1];  // leaf boxes tested box by box
+    h_totals[2] = (int64_t)h[4];  // leaf boxes tested with containment
+    h_totals[3] = (int64_t)h[5];  // hits emitted by contained slot ranges
   }
   return CRT_OK;
 }

@@ -278,8 +278,9 @@ def query(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, mode: int = _lib.CRT_QUERY_PE
 
 def query_stats(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, per_window: bool = False,
                 stream=None):
-    """Hit count and leaf boxes tested, in total (and per window)."""
-    tot = (ctypes.c_int64 * 2)()
+    """Hit count and leaf boxes tested (by the reference's algorithm, and with
+    the containment shortcut), in total (and per window)."""
+    tot = (ctypes.c_int64 * 4)()
     hits = tested = None
     if per_window and d_qbox.sz:
         hits = torch.empty(d_qbox.sz, dtype=torch.int64, device="cuda")
@@ -289,7 +290,8 @@ def query_stats(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, per_window: bool = Fals
                                      hits.data_ptr() if hits is not None else None,
                                      tested.data_ptr() if tested is not None else None, tot,
                                      _stream_handle(stream)), "query_stats")
-    out = {"hits": int(tot[0]), "tested": int(tot[1])}
+    out = {"hits": int(tot[0]), "tested": int(tot[1]), "tested_contain": int(tot[2]),
+           "range_hits": int(tot[3])}
     if per_window:
         out["per_window_hits"] = hits
         out["per_window_tested"] = tested

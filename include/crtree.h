@@ -215,10 +215,13 @@ int crt_query_plain_noalloc_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d
                                 const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
                                 int64_t capacity, crt_query_result* d_result, crt_stream_t stream);
 
-/* Per-window workload statistics: hit count and number of leaf boxes tested
- * (int64 device arrays of nq entries, either may be NULL); totals[0] = all
- * hits, totals[1] = all leaf boxes tested (host, may be NULL).  Synchronous.
- * Sizes outputs before a query and gives the benchmark its algorithmic bytes. */
+/* Per-window workload statistics: hit count and number of leaf boxes the
+ * reference's algorithm tests (int64 device arrays of nq entries, either may
+ * be NULL); totals (host, 4 entries, may be NULL): [0] all hits, [1] leaf
+ * boxes tested box by box (the reference's algorithm), [2] leaf boxes tested
+ * with the containment shortcut (this library's queries), [3] hits emitted
+ * as contained slot ranges.  Synchronous.  Sizes outputs before a query and
+ * gives the benchmark its algorithmic bytes. */
 int crt_query_stats_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                         const crt_bbox_f32* d_qbox, int64_t* d_hits, int64_t* d_tested,
                         int64_t* totals, crt_stream_t stream);

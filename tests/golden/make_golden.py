@@ -183,4 +183,6 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <outdir>")
+    main(sys.argv[1])

@@ -259,3 +259,24 @@ def test_query_matches_reference_golden(crt, path):
     dq = crt.BBox.from_host(q)
     want = (z["frontier_fid"], z["frontier_tid"])
     assert_all(all_forms(crt, d, rt, dq), want)
+
+
+def test_query_stats_match_oracle(crt):
+    """Per-window hit counts and leaf boxes tested by the reference's algorithm
+    equal the oracle's; the containment traversal tests no more boxes and
+    finds the same hits."""
+    b = D.clustered_boxes(400_000, seed=11, chunk=400_000)
+    q = D.mixed_windows(5_000, b, seed=12)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(16)
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    sb, t = O.build(b, 16)
+    want = O.tree_query_stats(t, sb, q)
+    st = crt.query_stats(rt, d, dq, per_window=True)
+    assert np.array_equal(st["per_window_hits"].cpu().numpy(), want.counts)
+    assert np.array_equal(st["per_window_tested"].cpu().numpy(), want.tested)
+    assert st["hits"] == int(want.counts.sum())
+    assert st["tested"] == int(want.tested.sum())
+    assert 0 <= st["tested_contain"] <= st["tested"]
+    assert 0 <= st["range_hits"] <= st["hits"]
