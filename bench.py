@@ -14,9 +14,13 @@ Headline (one JSON line on rank 0):
   e2e     the same query metric through the C ABI with host buffers: each step
           copies the windows from pinned host memory, queries, and copies every
           hit pair back to pinned host memory.
+  serving four resident trees (1M-50M boxes), 400 requests of 1-100k
+          windows arriving as a Poisson stream at 1k and 10k requests/s:
+          continuous batching against the plain form one request at a time,
+          windows/s and p50/p99 latency.
   roofline  of the dominant kernel (the persistent traversal): algorithmic bytes
-          16 B per window + 16 B per leaf box tested + 12 B per hit, over its
-          CUDA-event time, against the measured HBM copy bandwidth.
+          16 B per window + 16 B per leaf box it tests + 12 B per hit, over
+          its CUDA-event time, against the measured HBM copy bandwidth.
   cpu_baseline  the reference's own CPU brute force (nested_loop_query,
           compiled from its sources) on the host cores over a bounded sample.
 
@@ -65,8 +69,9 @@ def parse():
     p.add_argument("--autotune-windows", type=int, default=100_000)
     p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu,serve")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
-    p.add_argument("--serve-requests", type=int, default=300)
-    p.add_argument("--serve-rate", type=float, default=500.0)
+    p.add_argument("--serve-requests", type=int, default=400)
+    p.add_argument("--serve-rates", default="1000,10000",
+                   help="comma list of Poisson arrival rates (requests/s)")
     p.add_argument("--serve-max-batch", type=int, default=100_000)
     p.add_argument("--serve-arena-gb", type=int, default=64)
     return p.parse_args()
@@ -402,56 +407,31 @@ def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, d
 
 def serving_workload(args, rank):
     """Four device-resident trees (1M, 5M, 20M, 50M uniform boxes) and a
-    Poisson stream of requests: tree uniform, batch size log-uniform in
-    [1, 100k] windows, window side log-uniform in [1e-5, 1e-1]."""
+    request stream: tree uniform, batch size log-uniform in [1, 100k]
+    windows, window side log-uniform in [1e-5, 1e-1]; exponential
+    inter-arrival gaps of mean 1 (scaled by the rate)."""
     from curtree_b200 import datasets as D
     sizes = [int(x) for x in args.serve_trees.split(",")]
     trees = [D.uniform_boxes(n, seed=41 + i) for i, n in enumerate(sizes)]
     tree_idx, nq = D.serving_requests(args.serve_requests, len(trees), seed=104 + 1000 * rank,
                                       hi=args.serve_max_batch)
     rng = np.random.default_rng(204 + rank)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, args.serve_requests))
+    gaps = np.cumsum(rng.exponential(1.0, args.serve_requests))
     reqs = []
     for i in range(args.serve_requests):
         w = D.mixed_windows(int(nq[i]), trees[tree_idx[i]], seed=10_000 + 7 * i + 1000 * rank)
         reqs.append((int(tree_idx[i]), w))
-    return trees, reqs, arrivals
+    return trees, reqs, gaps
 
 
-def serving_leg(args, C, rank):
+def serve_run(srv, tids, reqs, arrivals):
+    """Replays one arrival schedule through the server; returns latencies
+    (arrival to completion), makespan, pairs and retries."""
     import time
-
-    import torch
-
-    from curtree_b200.server import Server
-    trees, reqs, arrivals = serving_workload(args, rank)
-    built = []
-    for b in trees:
-        d = C.BBox.from_host(b)
-        rt = C.RTree(args.fanout)
-        C.build_rtree(d, rt)
-        built.append((rt, d))
-    total_windows = sum(w.n for _, w in reqs)
-
-    # ---- served: continuous batching ------------------------------------------
-    srv = Server(arena_bytes=args.serve_arena_gb << 30, pairs_per_window=256.0)
-    tids = [srv.add_tree(rt, d) for rt, d in built]
-    # warm the device loop and the per-tree output estimates
-    for i in range(min(8, len(reqs))):
-        while srv.submit(tids[reqs[i][0]], reqs[i][1]) is None:
-            time.sleep(1e-3)
-    got = 0
-    while got < min(8, len(reqs)):
-        for c in srv.poll(wait_ms=50):
-            srv.release(c["request_id"])
-            got += 1
     lat = np.zeros(len(reqs))
-    pairs = 0
-    backlog = []
-    ids = {}
-    nxt = 0
-    done = 0
-    retries = 0
+    pairs = retries = 0
+    backlog, ids = [], {}
+    nxt = done = 0
     t0 = time.monotonic()
     while done < len(reqs):
         now = time.monotonic() - t0
@@ -476,24 +456,14 @@ def serving_leg(args, C, rank):
             done += 1
         if nxt < len(reqs) and not backlog:
             time.sleep(max(0.0, min(2e-4, arrivals[nxt] - (time.monotonic() - t0))))
-    makespan = time.monotonic() - t0
-    srv.close()
-    served = {"windows_per_s": total_windows / makespan, "requests_per_s": len(reqs) / makespan,
-              "p50_ms": float(np.percentile(lat, 50) * 1e3),
-              "p99_ms": float(np.percentile(lat, 99) * 1e3), "makespan_s": makespan,
-              "pairs": int(pairs), "retries": int(retries)}
+    return lat, time.monotonic() - t0, pairs, retries
 
-    # ---- plain: one request at a time, plain per-batch form ----------------------
-    stats = []
-    for ti, w in reqs:
-        dq = C.BBox.from_host(w)
-        stats.append(C.query_stats(built[ti][0], built[ti][1], dq)["hits"])
-    cap = max(max(stats), 1)
-    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
-    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
-    res = C.new_result_block()
-    h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
-    lat_p = np.zeros(len(reqs))
+
+def plain_run(C, built, reqs, arrivals, stats, fid, tid, res, h_res):
+    """The same schedule, one request at a time through the plain per-batch
+    form (count pass, scan, write pass)."""
+    import time
+    lat = np.zeros(len(reqs))
     t0 = time.monotonic()
     for i, (ti, w) in enumerate(reqs):
         wait = arrivals[i] - (time.monotonic() - t0)
@@ -504,17 +474,61 @@ def serving_leg(args, C, rank):
         h_res.copy_(res)
         r = C.read_result(h_res)
         assert r["count"] == stats[i], (r, stats[i])
-        lat_p[i] = time.monotonic() - (t0 + arrivals[i])
-    makespan_p = time.monotonic() - t0
-    plain = {"windows_per_s": total_windows / makespan_p, "requests_per_s": len(reqs) / makespan_p,
-             "p50_ms": float(np.percentile(lat_p, 50) * 1e3),
-             "p99_ms": float(np.percentile(lat_p, 99) * 1e3), "makespan_s": makespan_p}
-    assert served["pairs"] == sum(stats), (served["pairs"], sum(stats))
+        lat[i] = time.monotonic() - (t0 + arrivals[i])
+    return lat, time.monotonic() - t0
+
+
+def serving_leg(args, C, rank):
+    import time
+
+    import torch
+
+    from curtree_b200.server import Server
+    trees, reqs, gaps = serving_workload(args, rank)
+    built = []
+    for b in trees:
+        d = C.BBox.from_host(b)
+        rt = C.RTree(args.fanout)
+        C.build_rtree(d, rt)
+        built.append((rt, d))
+    total_windows = sum(w.n for _, w in reqs)
+    stats = []
+    for ti, w in reqs:
+        dq = C.BBox.from_host(w)
+        stats.append(C.query_stats(built[ti][0], built[ti][1], dq)["hits"])
+    cap = max(max(stats), 1)
+    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    res = C.new_result_block()
+    h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+
+    srv = Server(arena_bytes=args.serve_arena_gb << 30, pairs_per_window=256.0)
+    tids = [srv.add_tree(rt, d) for rt, d in built]
+    # warm the device loop and the per-tree output estimates
+    warm = min(8, len(reqs))
+    serve_run(srv, tids, reqs[:warm], np.zeros(warm))
+    summary = lambda lat, span: {
+        "windows_per_s": total_windows / span, "requests_per_s": len(reqs) / span,
+        "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "makespan_s": span}
+    rates = []
+    for rate in [float(x) for x in args.serve_rates.split(",")]:
+        arrivals = gaps / rate
+        lat, span, pairs, retries = serve_run(srv, tids, reqs, arrivals)
+        assert pairs == sum(stats), (pairs, sum(stats))
+        served = dict(summary(lat, span), pairs=int(pairs), retries=int(retries))
+        lat_p, span_p = plain_run(C, built, reqs, arrivals, stats, fid, tid, res, h_res)
+        plain = summary(lat_p, span_p)
+        rates.append({"rate_req_s": rate, "offered_windows_per_s": total_windows / arrivals[-1],
+                      "served": served, "plain": plain,
+                      "served_vs_plain_windows_per_s": served["windows_per_s"] / plain["windows_per_s"],
+                      "p99_served_le_plain": served["p99_ms"] <= plain["p99_ms"]})
+        time.sleep(0.05)
+    srv.close()
     return {"workload": f"trees {args.serve_trees} uniform boxes, fanout {args.fanout}; "
-                        f"{len(reqs)} requests, Poisson {args.serve_rate:g} req/s, batch "
+                        f"{len(reqs)} requests, Poisson arrivals, batch "
                         f"log-U[1, {args.serve_max_batch}] windows, side log-U[1e-5, 1e-1]",
-            "windows": int(total_windows), "served": served, "plain": plain,
-            "served_vs_plain_windows_per_s": served["windows_per_s"] / plain["windows_per_s"]}
+            "windows": int(total_windows), "pairs": int(sum(stats)), "rates": rates}
 
 
 def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):

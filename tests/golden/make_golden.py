@@ -31,9 +31,7 @@ sys.path.insert(0, ROOT)
 from curtree_b200 import datasets as D  # noqa: E402
 from curtree_b200.datasets import HostBoxes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
-
-REF = os.path.join(ROOT, "oracle", "_ref")
-
+from oracle import ref_gpu as R  # noqa: E402
 
 def boxes_from(xmin, ymin, xmax, ymax) -> HostBoxes:
     f = lambda a: np.asarray(a, np.float32)
@@ -102,27 +100,9 @@ def cases():
 
 
 def run(runner, mode, bfile, qfile, fanout, outdir):
-    os.makedirs(outdir, exist_ok=True)
-    cmd = [os.path.join(REF, runner), mode, bfile, qfile or "-", str(fanout), outdir, "1"]
-    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
-    if p.returncode != 0:
-        raise RuntimeError(f"{cmd} -> {p.returncode}\n{p.stdout[-2000:]}\n{p.stderr[-2000:]}")
-    line = [l for l in p.stdout.splitlines() if l.startswith("REFJSON ")][-1]
-    info = json.loads(line[len("REFJSON "):])
-    tree = np.fromfile(os.path.join(outdir, "tree.bin"), np.uint8)
-    rsz = int(tree[:8].view(np.int64)[0])
-    body = tree[16:]
-    arr = lambda k, dt: body[k * 4 * rsz:(k + 1) * 4 * rsz].view(dt)
-    t = {"xmin": arr(0, np.float32), "ymin": arr(1, np.float32), "xmax": arr(2, np.float32),
-         "ymax": arr(3, np.float32), "pos": arr(4, np.int32), "len": arr(5, np.int32)}
-    ids = np.fromfile(os.path.join(outdir, "sorted_ids.bin"), np.int32)
-    pairs = None
-    if mode == "query":
-        raw = np.fromfile(os.path.join(outdir, "pairs.bin"), np.uint8)
-        m = int(raw[:8].view(np.int64)[0])
-        fid = raw[8:8 + 4 * m].view(np.int32)
-        tid = raw[8 + 4 * m:8 + 8 * m].view(np.int32)
-        pairs = O.canonical_pairs(fid, tid)
+    t, ids, pairs, info = R.run(runner, mode, bfile, qfile, fanout, outdir, reps=1, timeout=600)
+    if pairs is not None:
+        pairs = O.canonical_pairs(*pairs)
     return t, ids, pairs, info
 
 
