@@ -67,7 +67,10 @@ def parse():
     p.add_argument("--sort-windows", type=int, default=1)
     p.add_argument("--autotune", type=int, default=1, help="pick fanout/warps/staging first (untimed)")
     p.add_argument("--autotune-windows", type=int, default=100_000)
-    p.add_argument("--skip", default="", help="comma list of legs to skip: build,e2e,plain,cpu,serve")
+    p.add_argument("--skip", default="",
+                   help="comma list of legs to skip: build,e2e,plain,cpu,serve,adversarial")
+    p.add_argument("--adv-boxes", type=int, default=50_000_000)
+    p.add_argument("--adv-windows", type=int, default=2_000_000)
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-rates", default="1000,10000",
@@ -357,6 +360,11 @@ def run_ours(args, rank, world, dist):
         out["serving"] = serving_leg(args, C, rank)
         torch.cuda.empty_cache()
 
+    # ---- adversarial geometry ------------------------------------------------------
+    if "adversarial" not in skip:
+        out["adversarial"] = adversarial_leg(args, C, stream, dist, world, rank)
+        torch.cuda.empty_cache()
+
     # ---- bulk load ------------------------------------------------------------
     if "build" not in skip:
         out["build"] = build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world)
@@ -531,6 +539,101 @@ def serving_leg(args, C, rank):
             "windows": int(total_windows), "pairs": int(sum(stats)), "rates": rates}
 
 
+def adversarial_leg(args, C, stream, dist, world, rank):
+    """Road-like boxes (centres on 100 segments, Pareto long sides capped at
+    0.5, aspect ratios up to 1e4) and a window mix of 50% points, 40% small
+    windows and 10% windows over 1% of the domain.  Batched: every window
+    through query_stream (one 2^30-pair output buffer reused, batches that
+    overflow re-run smaller); pairs are counted and dropped, as a consumer
+    that reduces them would.  Served: the first tenth of the windows as
+    requests of 1-1000 windows arriving at 1k requests/s."""
+    import time
+
+    import torch
+
+    from curtree_b200 import datasets as D
+    from curtree_b200.server import Server
+    b = D.road_boxes(args.adv_boxes, seed=5 + 1000 * rank)
+    q = D.road_windows(args.adv_windows, seed=105 + 1000 * rank)
+    d = C.BBox.from_host(b)
+    del b
+    rt = C.RTree(args.fanout)
+    C.build_rtree(d, rt)
+    dq = C.BBox.from_host(q)
+    total = C.query_stats(rt, d, dq)["hits"]
+    cap = C.query_capacity(1 << 30)
+    drop = lambda f, t, a: None
+    warm = C.BBox(dq.xmin[:20_000], dq.ymin[:20_000], dq.xmax[:20_000], dq.ymax[:20_000],
+                  dq.id[:20_000])
+    C.query_stream(rt, d, warm, drop, capacity=cap)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    st = C.query_stream(rt, d, dq, drop, capacity=cap, batch=1 << 16)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = reduce_max(e0.elapsed_time(e1), dist)
+    assert st["pairs"] == total, (st, total)
+    batched = {"windows_per_s": world * q.n / (ms / 1e3), "pairs_per_s": world * total / (ms / 1e3),
+               "ms": ms, "pairs": int(total), "batches": st["batches"], "retries": st["retries"],
+               "output_buffer_pairs": int(cap)}
+
+    # served
+    nserve = q.n // 10
+    rng = np.random.default_rng(7 + rank)
+    cuts = [0]
+    while cuts[-1] < nserve:
+        cuts.append(min(nserve, cuts[-1] + int(np.exp(rng.uniform(0, np.log(1000))))))
+    reqs = list(zip(cuts[:-1], cuts[1:]))
+    arrivals = np.cumsum(rng.exponential(1.0 / 1000.0, len(reqs)))
+    srv = Server(arena_bytes=args.serve_arena_gb << 30, pairs_per_window=256.0)
+    tree = srv.add_tree(rt, d)
+    windows = [C.BBox(dq.xmin[a:e], dq.ymin[a:e], dq.xmax[a:e], dq.ymax[a:e], dq.id[a:e])
+               for a, e in reqs]
+    lat = np.zeros(len(reqs))
+    backlog, ids = [], {}
+    nxt = done = 0
+    pairs = retries = 0
+    t0 = time.monotonic()
+    while done < len(reqs):
+        now = time.monotonic() - t0
+        while nxt < len(reqs) and arrivals[nxt] <= now:
+            backlog.append(nxt)
+            nxt += 1
+        while backlog:
+            rid = srv.submit(tree, windows[backlog[0]])
+            if rid is None:
+                break
+            ids[rid] = backlog.pop(0)
+        for c in srv.poll(max_out=256, wait_ms=0 if (backlog or nxt < len(reqs)) else 2):
+            i = ids.pop(c["request_id"])
+            if c["status"] != 0:
+                raise RuntimeError(f"served request failed: {c}")
+            lat[i] = c["complete_time_s"] - (t0 + arrivals[i])
+            pairs += c["count"]
+            retries += c["retries"]
+            srv.release(c["request_id"])
+            done += 1
+        if nxt < len(reqs) and not backlog:
+            time.sleep(max(0.0, min(2e-4, arrivals[nxt] - (time.monotonic() - t0))))
+    span = time.monotonic() - t0
+    srv.close()
+    served_total = C.query_stats(rt, d, C.BBox(dq.xmin[:nserve], dq.ymin[:nserve], dq.xmax[:nserve],
+                                                 dq.ymax[:nserve], dq.id[:nserve]))["hits"]
+    assert pairs == served_total, (pairs, served_total)
+    served = {"requests": len(reqs), "windows": int(nserve), "pairs": int(pairs),
+              "windows_per_s": nserve / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+              "p99_ms": float(np.percentile(lat, 99) * 1e3), "retries": int(retries),
+              "rate_req_s": 1000.0}
+    rt.free()
+    return {"workload": f"{args.adv_boxes // 1_000_000}M road boxes (100 segments, Pareto sides "
+                        f"capped at 0.5, aspect up to 1e4), {args.adv_windows // 1000}k windows "
+                        f"(50% points, 40% small, 10% over 1% of the domain), fanout {args.fanout}",
+            "batched": batched, "served": served}
+
+
 def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
     import torch
     from curtree_b200 import datasets as D
@@ -634,7 +737,7 @@ def main():
                 "roofline": out["roofline"], "cpu_baseline": cpu, "e2e": out.get("e2e"),
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
                 "plain": out.get("plain"), "build": out.get("build"),
-                "serving": out.get("serving"),
+                "serving": out.get("serving"), "adversarial": out.get("adversarial"),
                 "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                 "persistent_kernel_ms": p["kernel_ms"]}
         if "plain" in out:

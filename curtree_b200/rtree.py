@@ -276,6 +276,59 @@ def query(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, mode: int = _lib.CRT_QUERY_PE
     raise _lib.CrtError(_lib.CRT_ERR_OUTPUT_OVERFLOW, "query")
 
 
+def query_stream(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, consume, capacity: int = 1 << 30,
+                 batch: int = 1 << 16, mode: int = _lib.CRT_QUERY_PERSISTENT, stream=None,
+                 **opts) -> dict:
+    """Queries a window set whose pairs need not fit in memory at once: the
+    windows go through crt_query_into_f32 in consecutive batches against one
+    fixed output buffer of `capacity` pairs.  A batch that overflows is run
+    again on fewer windows (the result block reports the exact pair count it
+    needed, so the retry is sized from it); after a batch that used less than
+    half the buffer the next batch grows.  For each completed batch
+    `consume(fid, tid, first)` receives device views of its pairs (tid
+    relative to window `first`), before the buffer is reused.  A single
+    window with more than `capacity` pairs is CRT_ERR_OUTPUT_OVERFLOW.
+    Returns {"pairs", "batches", "retries"}."""
+    nq = d_qbox.sz
+    cap = int(capacity)
+    # pairs a batch may need and still fit: the persistent form reserves
+    # output in per-warp chunks, which may leave one partly used chunk each
+    usable = cap - query_capacity(0, mode)
+    if usable <= 0:
+        raise _lib.CrtError(_lib.CRT_ERR_INVALID_ARG,
+                            f"query_stream: capacity {cap} is below the form's slack")
+    fid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    tid = torch.empty(cap, dtype=torch.int32, device="cuda")
+    res = new_result_block()
+    h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+    st = {"pairs": 0, "batches": 0, "retries": 0}
+    a, size = 0, max(1, int(batch))
+    while a < nq:
+        b = min(nq, a + size)
+        sub = BBox(d_qbox.xmin[a:b], d_qbox.ymin[a:b], d_qbox.xmax[a:b], d_qbox.ymax[a:b],
+                   d_qbox.id[a:b])
+        query_into(d_rt, d_rbox, sub, fid, tid, res, None, mode, stream, **opts)
+        h_res.copy_(res)
+        r = read_result(h_res)
+        if r["error"]:
+            raise _lib.CrtError(r["error"], "query_stream")
+        if r["overflow"]:
+            st["retries"] += 1
+            if b - a == 1:
+                raise _lib.CrtError(_lib.CRT_ERR_OUTPUT_OVERFLOW,
+                                    f"query_stream: window {a} alone has {r['required']} pairs")
+            size = max(1, min(b - a - 1, int((b - a) * 0.85 * usable / max(r["required"], 1))))
+            continue
+        n = r["count"]
+        consume(fid[:n], tid[:n], a)
+        st["pairs"] += n
+        st["batches"] += 1
+        a = b
+        if 2 * n < usable:
+            size = min(max(int(batch), 1) * 64, 2 * size)
+    return st
+
+
 def query_stats(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, per_window: bool = False,
                 stream=None):
     """Hit count and leaf boxes tested (by the reference's algorithm, and with
