@@ -1206,7 +1206,7 @@ int plan_launch(void* hp, cudaStream_t stream)
   Plan* p = (Plan*)hp;
   cudaError_t e = cudaGraphLaunch(p->exec[0], stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
-  CRT_LAUNCHED(p->sort ? 7 : 0);
+  CRT_LAUNCHED(p->sort ? 6 : 0);  // window keys, sort plan, four sort passes
   launch_traverse(p->traverse, stream);
   e = cudaGraphLaunch(p->exec[1], stream);
   CRT_LAUNCHED(3);
