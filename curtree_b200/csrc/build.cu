@@ -144,19 +144,52 @@ __device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift)
   return (k >> shift) & 0xFFu;
 }
 
-// Lanes of the warp whose value equals this lane's (v < 512), from one ballot
-// per bit; on this part it issues faster than __match_any_sync (measured over
-// the four passes of a 100M-key build: 3.7 ms against 4.3 ms).
+// Lanes of the warp whose value equals this lane's (v < 2^kBits), from one
+// ballot per bit; on this part it issues faster than __match_any_sync
+// (measured over the four passes of a 100M-key build: 3.7 ms against 4.3 ms).
+template <int kBits>
 __device__ __forceinline__ uint32_t peer_mask(uint32_t v)
 {
   uint32_t peers = 0xffffffffu;
 #pragma unroll
-  for (int b = 0; b < 9; b++) {
+  for (int b = 0; b < kBits; b++) {
     const bool bit = (v >> b) & 1u;
     const uint32_t bal = __ballot_sync(0xffffffffu, bit);
     peers &= bit ? bal : ~bal;
   }
   return peers;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared memory of one pass: (key, slot) pairs staged in destination order,
+// the tile's incoming slots (prefetched while the tile is ranked), and the
+// per-warp digit counters (16-bit: at most 8192 per tile).
+constexpr size_t kSortSmem = (size_t)kSortTile * 8 + (size_t)kSortTile * 4 +
+                             (size_t)kSortWarps * kBins * 2;
+
+// Ranks this thread's keys inside its warp, stably (rounds in order, lanes in
+// order).  kFull: every item of the tile is valid (no bounds checks, and the
+// digit fits 8 bits, so 8 ballots); otherwise invalid items take digit 256.
+template <bool kFull>
+__device__ __forceinline__ void rank_keys(const uint32_t (&key)[kSortIpt], uint32_t (&rank)[kSortIpt],
+                                          uint16_t* wh, int wbase, int tile_n, int shift)
+{
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kSortIpt; i++) {
+    const bool v = kFull || wbase + 32 * i < tile_n;
+    const uint32_t dig = v ? digit_of(key[i], shift) : kBins;
+    const uint32_t peers = kFull ? peer_mask<8>(dig) : peer_mask<9>(dig);
+    const uint32_t old = v ? wh[dig] : 0u;
+    __syncwarp();
+    if (v && (peers & lt) == 0) wh[dig] = (uint16_t)(old + __popc(peers));
+    __syncwarp();
+    rank[i] = old + __popc(peers & lt);
+  }
 }
 
 // One stable LSD pass over (key, slot) pairs for the 8-bit digit at `digit`.
@@ -165,10 +198,10 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     onesweep_kernel(int digit, SortBufs bufs, int64_t n64, uint64_t* __restrict__ status,
                     BuildCtrl* __restrict__ ctrl, int flags)
 {
-  extern __shared__ uint32_t smem[];
-  uint32_t* s_keys = smem;                   // kSortTile
-  uint32_t* s_vals = smem + kSortTile;       // kSortTile
-  uint32_t* s_whist = smem + 2 * kSortTile;  // kSortWarps x kBins: counts, then offsets
+  extern __shared__ __align__(16) unsigned char smem[];
+  uint2* s_kv = (uint2*)smem;                                       // kSortTile
+  uint32_t* s_vin = (uint32_t*)(smem + (size_t)kSortTile * 8);      // kSortTile
+  uint16_t* s_whist = (uint16_t*)(smem + (size_t)kSortTile * 12);   // kSortWarps x kBins
   __shared__ int s_gbase[kBins];
   __shared__ int s_tile;
   __shared__ int s_wsum[kBins / 32];
@@ -184,7 +217,7 @@ __global__ void __launch_bounds__(kSortThreads, 2)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(&ctrl->tile_ctr[digit], 1);
-  for (int i = tid; i < kSortWarps * kBins; i += kSortThreads) s_whist[i] = 0;
+  for (int i = tid; i < kSortWarps * kBins / 2; i += kSortThreads) ((uint32_t*)s_whist)[i] = 0;
   __syncthreads();
   const int tile = s_tile;
   const int base = tile * kSortTile;
@@ -195,27 +228,37 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   uint32_t* __restrict__ dst_v = bufs.vals[parity ^ 1];
   const int wbase = warp * 32 * kSortIpt + lane;  // this lane's first item in the tile
 
+  // the tile's incoming slots land in shared memory while the keys are ranked
+  // (16-byte async copies; the tile start is 32 KiB-aligned)
+  if (!first) {
+#pragma unroll
+    for (int c = tid; c < kSortTile / 4; c += kSortThreads) {
+      const int left = tile_n - 4 * c;
+      if (left > 0) {
+        const int bytes = min(left, 4) * 4;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(s_vin + 4 * c)),
+                     "l"(src_v + 4 * c), "r"(bytes)
+                     : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+
   // load keys (warp-striped: item i of a lane is wbase + 32 i)
   uint32_t key[kSortIpt];
   uint32_t rank[kSortIpt];
+  uint16_t* wh = s_whist + warp * kBins;
+  if (tile_n == kSortTile) {
 #pragma unroll
-  for (int i = 0; i < kSortIpt; i++) {
-    const int j = wbase + 32 * i;
-    key[i] = j < tile_n ? src_k[j] : 0u;
-  }
-  // rank inside the warp, stably: rounds in order, lanes in order
-  uint32_t* wh = s_whist + warp * kBins;
-  const uint32_t lt = lanemask_lt();
+    for (int i = 0; i < kSortIpt; i++) key[i] = src_k[wbase + 32 * i];
+    rank_keys<true>(key, rank, wh, wbase, tile_n, shift);
+  } else {
 #pragma unroll
-  for (int i = 0; i < kSortIpt; i++) {
-    const bool v = wbase + 32 * i < tile_n;
-    const uint32_t dig = v ? digit_of(key[i], shift) : kBins;
-    const uint32_t peers = peer_mask(dig);
-    const uint32_t old = v ? wh[dig] : 0u;
-    __syncwarp();
-    if (v && (peers & lt) == 0) wh[dig] = old + __popc(peers);
-    __syncwarp();
-    rank[i] = old + __popc(peers & lt);
+    for (int i = 0; i < kSortIpt; i++) {
+      const int j = wbase + 32 * i;
+      key[i] = j < tile_n ? src_k[j] : 0u;
+    }
+    rank_keys<false>(key, rank, wh, wbase, tile_n, shift);
   }
   __syncthreads();
   // per bin: exclusive prefix over warps, the tile count, and the tile-local bin start
@@ -225,7 +268,7 @@ __global__ void __launch_bounds__(kSortThreads, 2)
 #pragma unroll
     for (int w = 0; w < kSortWarps; w++) {
       const int c = (int)s_whist[w * kBins + tid];
-      s_whist[w * kBins + tid] = run;
+      s_whist[w * kBins + tid] = (uint16_t)run;
       run += c;
     }
     cnt = run;
@@ -244,7 +287,8 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     for (int w = 0; w < warp; w++) binstart += s_wsum[w];
     // fold the bin start into every warp's offset: one lookup per key later
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) s_whist[w * kBins + tid] += binstart;
+    for (int w = 0; w < kSortWarps; w++)
+      s_whist[w * kBins + tid] = (uint16_t)(s_whist[w * kBins + tid] + binstart);
 
     // decoupled look-back for bin `tid`
     int excl = 0;
@@ -273,25 +317,25 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     }
     s_gbase[tid] = ctrl->bucket_start[digit * kBins + tid] + excl - binstart;
   }
+  if (!first) asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
-  // stage keys and slots in the order of their destination
+  // stage (key, slot) pairs in the order of their destination
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
     const int j = wbase + 32 * i;
     if (j < tile_n) {
       const int pos = (int)(wh[digit_of(key[i], shift)] + rank[i]);
-      s_keys[pos] = key[i];
-      s_vals[pos] = first ? (uint32_t)(base + j) : src_v[j];
+      s_kv[pos] = make_uint2(key[i], first ? (uint32_t)(base + j) : s_vin[j]);
     }
   }
   __syncthreads();
   for (int j = tid; j < tile_n; j += kSortThreads) {
-    const uint32_t k = s_keys[j];
-    const int dst = s_gbase[digit_of(k, shift)] + j;
+    const uint2 kv = s_kv[j];
+    const int dst = s_gbase[digit_of(kv.x, shift)] + j;
     if ((uint32_t)dst < (uint32_t)n) {
-      if (!last) dst_k[dst] = k;
-      dst_v[dst] = s_vals[j];
+      if (!last) dst_k[dst] = kv.x;
+      dst_v[dst] = kv.y;
     }
   }
 }
@@ -441,7 +485,7 @@ void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream
   SortCtrl* ctrl = sort_ctrl(zero_block);
   uint64_t* status = sort_status(zero_block);
   plan_kernel<<<1, 128, 0, stream>>>(sort_hist(zero_block), n, ctrl);
-  const size_t smem = (2 * kSortTile + kSortWarps * kBins) * sizeof(uint32_t);
+  const size_t smem = kSortSmem;
   cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   for (int d = 0; d < 4; d++) {
     ProfScope ps("sort_pass", stream);

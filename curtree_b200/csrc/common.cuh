@@ -114,6 +114,23 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p)
   return v;
 }
 
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_ull(const unsigned long long* p)
+{
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // Upper bound on polls of any device-side wait before it gives up, records
 // CRT_ERR_DEVICE_TIMEOUT and returns (about a second with the back-off).
 constexpr uint32_t kSpinLimit = 1u << 22;

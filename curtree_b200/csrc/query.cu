@@ -46,10 +46,17 @@ struct QueryCounters {
   unsigned long long next;    // next unreserved output slot
   unsigned long long hits;    // exact pair count
   unsigned long long nholes;  // unused chunk ends recorded
+  unsigned long long jobs_tail;  // range pieces reserved in the job queue (persistent)
+  unsigned long long jobs_head;  // range pieces taken
+  unsigned long long active;     // warps inside a window's traversal (persistent)
   int error;
   int pad;
   unsigned long long nq;      // window count (read by graph replays)
 };
+
+// query_stats and the allocation-free entry point keep the counters in the
+// first 256 bytes of their scratch.
+static_assert(sizeof(QueryCounters) <= 256, "counters fit their scratch slot");
 
 struct Hole {
   long long start;
@@ -105,17 +112,85 @@ struct OffsetEmit {
   }
   __device__ __forceinline__ void range(const int* bid, long long first, long long count)
   {
-    const int lane = (int)lane_id();
-    for (long long i = lane; i < count; i += 32) {
-      const long long slot = base + i;
-      if (slot < cap) {
-        fid[slot] = __ldg(bid + first + i);
-        tid[slot] = q;
-      }
-    }
+    copy_range(bid, first, count, fid, tid, base, cap, q);
     base += count;
   }
 };
+
+// ---------------------------------------------------------------------------
+// Range sharing (persistent form).  One window can own a contained subtree of
+// millions of boxes; copying it with one warp would leave the rest of the GPU
+// idle at the end of a batch.  The warp that finds such a range reserves its
+// output, cuts it into kPiece-id pieces, publishes them in a job queue and
+// goes on with its window.  Warps take pieces before each new window and
+// before they leave, and a warp leaves only when the queue is empty (or no
+// window is in progress any more), so every published piece is copied; a
+// taker waits, bounded, only for the few stores that publish its piece.
+// ---------------------------------------------------------------------------
+struct RangeJob {
+  long long first;  // first sorted slot
+  long long slot;   // first output slot
+  int count;
+  int q;
+  unsigned ready;   // 1 once published; the taker clears it
+  int pad;
+};
+constexpr int kJobs = 1 << 16;      // queue entries per launch (2 MiB)
+constexpr int kPiece = 8192;        // ids per piece
+constexpr int kShareMin = 4 * kPiece;  // ranges shorter than this stay with their finder
+
+// Takes the next published-or-reserved piece; -1 when the queue is empty
+// (warp-collective).
+__device__ __forceinline__ long long take_job(QueryCounters* ctr)
+{
+  long long h = -1;
+  if (lane_id() == 0) {
+    while (true) {
+      const unsigned long long hh = ld_relaxed_ull(&ctr->jobs_head);
+      const unsigned long long t = min(ld_relaxed_ull(&ctr->jobs_tail), (unsigned long long)kJobs);
+      if (hh >= t) break;
+      if (atomicCAS(&ctr->jobs_head, hh, hh + 1) == hh) {
+        h = (long long)hh;
+        break;
+      }
+    }
+  }
+  return __shfl_sync(0xffffffffu, h, 0);
+}
+
+// Copies piece `h` once its publisher has written it (warp-collective).
+__device__ __forceinline__ void run_job(RangeJob* jobs, long long h, const int* bid,
+                                        int32_t* fid, int32_t* tid, long long cap, int* err)
+{
+  RangeJob* J = jobs + h;
+  long long first = 0, slot = 0;
+  int count = 0, q = 0, ok = 0;
+  if (lane_id() == 0) {
+    for (uint32_t spin = 0; spin < kSpinLimit; spin++) {
+      if (ld_acquire_u32(&J->ready)) {
+        ok = 1;
+        break;
+      }
+      if (spin > 32) __nanosleep(64);
+    }
+    if (ok) {
+      first = J->first;
+      slot = J->slot;
+      count = J->count;
+      q = J->q;
+      J->ready = 0;
+    } else {
+      raise_error(err, CRT_ERR_DEVICE_TIMEOUT);
+    }
+  }
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (!ok) return;
+  first = __shfl_sync(0xffffffffu, first, 0);
+  slot = __shfl_sync(0xffffffffu, slot, 0);
+  count = __shfl_sync(0xffffffffu, count, 0);
+  q = __shfl_sync(0xffffffffu, q, 0);
+  copy_range(bid, first, count, fid, tid, slot, cap, q);
+}
 
 // Warp-reserved output chunks (persistent form).
 struct ChunkEmit {
@@ -128,6 +203,8 @@ struct ChunkEmit {
   long long hits = 0;
   int chunk;
   int q;
+  RangeJob* jobs = nullptr;  // null: no range sharing
+  QueryCounters* ctr = nullptr;
   __device__ __forceinline__ void begin(int qq) { q = qq; }
   __device__ __forceinline__ void operator()(bool hit, int id)
   {
@@ -166,13 +243,28 @@ struct ChunkEmit {
     if (lane_id() == 0) nb = atomicAdd(next, (unsigned long long)count);
     nb = __shfl_sync(0xffffffffu, nb, 0);
     hits += count;
-    for (long long i = lane_id(); i < count; i += 32) {
-      const long long slot = (long long)nb + i;
-      if (slot < cap) {
-        fid[slot] = __ldg(bid + first + i);
-        tid[slot] = q;
-      }
+    if (!jobs || count < kShareMin) {
+      copy_range(bid, first, count, fid, tid, (long long)nb, cap, q);
+      return;
     }
+    // publish the pieces; the ones the queue has no room for are copied here
+    const long long np = (count + kPiece - 1) / kPiece;
+    unsigned long long j0 = 0;
+    if (lane_id() == 0) j0 = atomicAdd(&ctr->jobs_tail, (unsigned long long)np);
+    j0 = __shfl_sync(0xffffffffu, j0, 0);
+    const long long own = max(0ll, min(np, (long long)kJobs - (long long)j0));
+    for (long long p = lane_id(); p < own; p += 32) {
+      const long long j = (long long)j0 + p;
+      const long long off = p * kPiece;
+      jobs[j].first = first + off;
+      jobs[j].slot = (long long)nb + off;
+      jobs[j].count = (int)min((long long)kPiece, count - off);
+      jobs[j].q = q;
+      st_release_u32(&jobs[j].ready, 1u);
+    }
+    if (own < np)
+      copy_range(bid, first + own * kPiece, count - own * kPiece, fid, tid,
+                 (long long)nb + own * kPiece, cap, q);
   }
 };
 
@@ -340,6 +432,7 @@ struct PersistParams {
   QueryCounters* ctr;
   Hole* holes;
   long long max_holes;
+  RangeJob* jobs;  // kJobs entries, ready flags zeroed before the launch
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -358,7 +451,10 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
-template <int kThreads, int kMinBlocks>
+// kShare: range sharing (the job queue).  Its code needs registers the
+// tighter CTA shapes do not have, so only the 8-warp shape (64 registers)
+// shares ranges; the autotuner weighs the shapes against each other.
+template <int kThreads, int kMinBlocks, bool kShare>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
     persistent_kernel(PersistParams P)
 {
@@ -433,10 +529,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   emit.cap = P.cap;
   emit.next = &P.ctr->next;
   emit.chunk = P.chunk;
+  emit.jobs = kShare ? P.jobs : nullptr;
+  emit.ctr = P.ctr;
   (void)warps;
   while (true) {
+    // pieces of other windows' contained ranges first
+    const long long h = (kShare && P.jobs) ? take_job(P.ctr) : -1;
+    if (h >= 0) {
+      run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
+      continue;
+    }
     unsigned long long t = 0;
-    if (lane_id() == 0) t = atomicAdd(&P.ctr->ticket, 1ull);
+    if (lane_id() == 0) {
+      t = atomicAdd(&P.ctr->ticket, 1ull);
+      if (kShare && (long long)t < nq) atomicAdd(&P.ctr->active, 1ull);
+    }
     t = __shfl_sync(0xffffffffu, t, 0);
     if ((long long)t >= nq) break;
     int q = order ? (int)order[t] : (int)t;
@@ -444,6 +551,26 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     emit.begin(q);
     traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
              P.stack_cap, emit, &P.ctr->error);
+    if (kShare) {
+      __syncwarp();
+      if (lane_id() == 0) atomicAdd(&P.ctr->active, ~0ull);  // -1
+    }
+  }
+  // No windows left: while other warps are still inside windows, stay to take
+  // the pieces they may publish.  Leaving is always safe (a finder drains its
+  // own pieces), so the wait is bounded and ends without an error.
+  if (kShare && P.jobs) {
+    for (uint32_t spin = 0; spin < kSpinLimit; spin++) {
+      const long long h = take_job(P.ctr);
+      if (h >= 0) {
+        run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
+        continue;
+      }
+      int busy = 0;
+      if (lane_id() == 0) busy = ld_relaxed_ull(&P.ctr->active) != 0;
+      if (!__shfl_sync(0xffffffffu, busy, 0)) break;
+      __nanosleep(1000);
+    }
   }
   if (lane_id() == 0) {
     if (emit.hits) atomicAdd(&P.ctr->hits, (unsigned long long)emit.hits);
@@ -670,9 +797,9 @@ struct PersistVariant {
 };
 
 static const PersistVariant kVariants[] = {
-    {1024, 2, (const void*)persistent_kernel<1024, 2>},  // 64 warps/SM, 32 registers
-    {512, 3, (const void*)persistent_kernel<512, 3>},    // 48 warps/SM, 40 registers
-    {256, 4, (const void*)persistent_kernel<256, 4>},    // 32 warps/SM, 64 registers
+    {1024, 2, (const void*)persistent_kernel<1024, 2, false>},  // 64 warps/SM, 32 registers
+    {512, 3, (const void*)persistent_kernel<512, 3, false>},    // 48 warps/SM, 40 registers
+    {256, 4, (const void*)persistent_kernel<256, 4, true>},     // 32 warps/SM, 64 registers
 };
 
 static const PersistVariant& variant_for(int warps_per_cta)
@@ -731,6 +858,7 @@ struct PersistScratch {
   void* sort_zero;
   SortBufs bufs;
   long long max_holes;
+  RangeJob* jobs;
   size_t bytes;
 };
 
@@ -738,7 +866,7 @@ static size_t persist_scratch_bytes(int64_t max_nq, long long max_holes, bool so
 {
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   size_t b = al(sizeof(QueryCounters)) + 2 * al(sizeof(Hole) * max_holes) +
-             al(sizeof(long long) * (max_holes + 1));
+             al(sizeof(long long) * (max_holes + 1)) + al(sizeof(RangeJob) * kJobs);
   if (sort) b += al(sort_zero_bytes(max_nq)) + 4 * al(4 * (size_t)std::max<int64_t>(max_nq, 1));
   return b;
 }
@@ -752,6 +880,7 @@ static void persist_scratch_carve(char* base, int64_t max_nq, long long max_hole
   S.holes = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
   S.sorted = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
   S.cum = (long long*)(base + off); off += al(sizeof(long long) * (max_holes + 1));
+  S.jobs = (RangeJob*)(base + off); off += al(sizeof(RangeJob) * kJobs);
   S.sort_zero = nullptr;
   if (sort) {
     S.sort_zero = base + off; off += al(sort_zero_bytes(max_nq));
@@ -773,8 +902,9 @@ static void persist_scratch_carve(char* base, int64_t max_nq, long long max_hole
 static void enqueue_pre(const WindowView& W, int64_t max_nq, const PersistScratch& S, bool sort,
                         cudaStream_t stream)
 {
-  // counters (keep nq) and the sort's zeroed block
+  // counters (keep nq), the job queue's ready flags and the sort's zeroed block
   cudaMemsetAsync(S.ctr, 0, offsetof(QueryCounters, nq), stream);
+  cudaMemsetAsync(S.jobs, 0, sizeof(RangeJob) * kJobs, stream);
   if (sort && max_nq > 0) {
     const int sms = sm_count();
     cudaMemsetAsync(S.sort_zero, 0, sort_zero_bytes(max_nq), stream);
@@ -817,6 +947,7 @@ static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
   P.ctr = S.ctr;
   P.holes = S.holes;
   P.max_holes = S.max_holes;
+  P.jobs = S.jobs;
   L.smem = ps.smem;
   L.threads = ps.v->threads;
   L.fn = ps.v->fn;

@@ -150,13 +150,7 @@ struct StagedEmit {
     unsigned long long b = 0;
     if (lane_id() == 0) b = atomicAdd(&ctr->next, (unsigned long long)count);
     b = __shfl_sync(0xffffffffu, b, 0);
-    for (long long i = lane_id(); i < count; i += 32) {
-      const long long slot = (long long)b + i;
-      if (slot < cap) {
-        fid[slot] = __ldg(bid + first + i);
-        tid[slot] = q;
-      }
-    }
+    copy_range(bid, first, count, fid, tid, (long long)b, cap, q);
   }
   __device__ __forceinline__ void operator()(bool hit, int id)
   {

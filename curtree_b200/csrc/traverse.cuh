@@ -125,6 +125,66 @@ __device__ __forceinline__ void emit_range_default(Emit& emit, const int* __rest
   }
 }
 
+// Writes the pairs (bid[first + i], q) to output slots slot0 + i for
+// i < count, skipping slots at or past `cap` (warp-collective).  A contained
+// subtree can hold millions of boxes, so the ids are read as 16-byte vectors
+// (128 ids per warp step, kRangeUnroll steps in flight) instead of one 4-byte
+// load per lane; one step keeps the persistent kernels within their register
+// budgets.
+constexpr int kRangeUnroll = 1;
+
+__device__ __forceinline__ void put_pair(int32_t* __restrict__ fid, int32_t* __restrict__ tid,
+                                         long long slot, long long cap, int id, int q)
+{
+  if (slot < cap) {
+    fid[slot] = id;
+    tid[slot] = q;
+  }
+}
+
+__device__ __forceinline__ void copy_range(const int* __restrict__ bid, long long first,
+                                           long long count, int32_t* __restrict__ fid,
+                                           int32_t* __restrict__ tid, long long slot0,
+                                           long long cap, int q)
+{
+  const int lane = (int)lane_id();
+  const int* src = bid + first;
+  // head: ids before the first 16-byte boundary of the source
+  long long head = (long long)((4 - (((uintptr_t)src >> 2) & 3)) & 3);
+  if (head > count) head = count;
+  if (lane < head) put_pair(fid, tid, slot0 + lane, cap, __ldg(src + lane), q);
+  const int4* v = reinterpret_cast<const int4*>(src + head);
+  const long long nv = (count - head) >> 2;
+  const long long s = slot0 + head;
+  for (long long g0 = 0; g0 < nv; g0 += 32 * kRangeUnroll) {
+    int4 r[kRangeUnroll];
+#pragma unroll
+    for (int u = 0; u < kRangeUnroll; u++) {
+      const long long g = g0 + u * 32 + lane;
+      if (g < nv) r[u] = __ldg(v + g);
+    }
+#pragma unroll
+    for (int u = 0; u < kRangeUnroll; u++) {
+      const long long g = g0 + u * 32 + lane;
+      if (g < nv) {
+        const long long sl = s + 4 * g;
+        if (sl + 3 < cap && ((((uintptr_t)(fid + sl)) | ((uintptr_t)(tid + sl))) & 15) == 0) {
+          *reinterpret_cast<int4*>(fid + sl) = r[u];
+          *reinterpret_cast<int4*>(tid + sl) = make_int4(q, q, q, q);
+        } else {
+          put_pair(fid, tid, sl + 0, cap, r[u].x, q);
+          put_pair(fid, tid, sl + 1, cap, r[u].y, q);
+          put_pair(fid, tid, sl + 2, cap, r[u].z, q);
+          put_pair(fid, tid, sl + 3, cap, r[u].w, q);
+        }
+      }
+    }
+  }
+  // tail: the last (count - head) % 4 ids
+  const long long done = head + 4 * nv;
+  if (lane < count - done) put_pair(fid, tid, slot0 + done + lane, cap, __ldg(src + done + lane), q);
+}
+
 template <class Emit, bool kContain = true>
 __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, int K,
                                          int lane_g, int lane_c, float x1, float y1, float x2,

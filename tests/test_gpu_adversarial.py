@@ -99,7 +99,7 @@ def test_streamed_batches_with_overflow_and_retry(env, mode):
     cap = C.query_capacity(4_000_000, m)  # room for 4M pairs a batch
     dq = C.BBox.from_host(q)
     dg = Digest(q.n)
-    st = C.query_stream(rt, d, dq, dg.add, capacity=cap, batch=4096, mode=m)
+    st = C.query_stream(rt, d, dq, dg.add, capacity=cap, batch=1 << 16, mode=m)
     assert st["retries"] > 0 and st["batches"] > 10
     assert st["pairs"] == int(want.counts.sum())
     dg.check(want)
