@@ -46,9 +46,6 @@ struct QueryCounters {
   unsigned long long next;    // next unreserved output slot
   unsigned long long hits;    // exact pair count
   unsigned long long nholes;  // unused chunk ends recorded
-  unsigned long long jobs_tail;  // range pieces reserved in the job queue (persistent)
-  unsigned long long jobs_head;  // range pieces taken
-  unsigned long long active;     // warps inside a window's traversal (persistent)
   int error;
   int pad;
   unsigned long long nq;      // window count (read by graph replays)
@@ -135,34 +132,48 @@ struct RangeJob {
   unsigned ready;   // 1 once published; the taker clears it
   int pad;
 };
-constexpr int kJobs = 1 << 16;      // queue entries per launch (2 MiB)
-constexpr int kPiece = 8192;        // ids per piece
-constexpr int kShareMin = 4 * kPiece;  // ranges shorter than this stay with their finder
+// The queue's counters, each on its own 128-byte line: idle warps poll them,
+// and they must not share a line with the ticket and output counters every
+// busy warp updates.
+struct JobQueue {
+  unsigned long long tail;  // pieces reserved
+  unsigned long long pad0[15];
+  unsigned long long head;  // pieces taken
+  unsigned long long pad1[15];
+  unsigned long long active;  // warps inside a window's traversal
+  unsigned long long pad2[15];
+  RangeJob entries[1];  // kJobs
+};
+constexpr int kJobs = 1 << 18;         // queue entries per launch (8 MiB)
+constexpr int kPiece = 16384;          // ids per piece
+constexpr int kShareMin = 2 * kPiece;  // ranges shorter than this stay with their finder
+constexpr size_t kJobQueueBytes = offsetof(JobQueue, entries) + sizeof(RangeJob) * kJobs;
 
 // Takes the next published-or-reserved piece; -1 when the queue is empty
 // (warp-collective).
-__device__ __forceinline__ long long take_job(QueryCounters* ctr)
+__device__ __forceinline__ long long take_job(JobQueue* Q)
 {
   long long h = -1;
   if (lane_id() == 0) {
-    while (true) {
-      const unsigned long long hh = ld_relaxed_ull(&ctr->jobs_head);
-      const unsigned long long t = min(ld_relaxed_ull(&ctr->jobs_tail), (unsigned long long)kJobs);
+    for (int attempt = 0;; attempt++) {
+      const unsigned long long hh = ld_relaxed_ull(&Q->head);
+      const unsigned long long t = min(ld_relaxed_ull(&Q->tail), (unsigned long long)kJobs);
       if (hh >= t) break;
-      if (atomicCAS(&ctr->jobs_head, hh, hh + 1) == hh) {
+      if (atomicCAS(&Q->head, hh, hh + 1) == hh) {
         h = (long long)hh;
         break;
       }
+      __nanosleep(32u << min(attempt, 5));  // lost the race: back off
     }
   }
   return __shfl_sync(0xffffffffu, h, 0);
 }
 
 // Copies piece `h` once its publisher has written it (warp-collective).
-__device__ __forceinline__ void run_job(RangeJob* jobs, long long h, const int* bid,
+__device__ __forceinline__ void run_job(JobQueue* Q, long long h, const int* bid,
                                         int32_t* fid, int32_t* tid, long long cap, int* err)
 {
-  RangeJob* J = jobs + h;
+  RangeJob* J = Q->entries + h;
   long long first = 0, slot = 0;
   int count = 0, q = 0, ok = 0;
   if (lane_id() == 0) {
@@ -203,8 +214,7 @@ struct ChunkEmit {
   long long hits = 0;
   int chunk;
   int q;
-  RangeJob* jobs = nullptr;  // null: no range sharing
-  QueryCounters* ctr = nullptr;
+  JobQueue* jobs = nullptr;  // null: no range sharing
   __device__ __forceinline__ void begin(int qq) { q = qq; }
   __device__ __forceinline__ void operator()(bool hit, int id)
   {
@@ -250,17 +260,17 @@ struct ChunkEmit {
     // publish the pieces; the ones the queue has no room for are copied here
     const long long np = (count + kPiece - 1) / kPiece;
     unsigned long long j0 = 0;
-    if (lane_id() == 0) j0 = atomicAdd(&ctr->jobs_tail, (unsigned long long)np);
+    if (lane_id() == 0) j0 = atomicAdd(&jobs->tail, (unsigned long long)np);
     j0 = __shfl_sync(0xffffffffu, j0, 0);
     const long long own = max(0ll, min(np, (long long)kJobs - (long long)j0));
     for (long long p = lane_id(); p < own; p += 32) {
-      const long long j = (long long)j0 + p;
+      RangeJob& J = jobs->entries[(long long)j0 + p];
       const long long off = p * kPiece;
-      jobs[j].first = first + off;
-      jobs[j].slot = (long long)nb + off;
-      jobs[j].count = (int)min((long long)kPiece, count - off);
-      jobs[j].q = q;
-      st_release_u32(&jobs[j].ready, 1u);
+      J.first = first + off;
+      J.slot = (long long)nb + off;
+      J.count = (int)min((long long)kPiece, count - off);
+      J.q = q;
+      st_release_u32(&J.ready, 1u);
     }
     if (own < np)
       copy_range(bid, first + own * kPiece, count - own * kPiece, fid, tid,
@@ -432,7 +442,7 @@ struct PersistParams {
   QueryCounters* ctr;
   Hole* holes;
   long long max_holes;
-  RangeJob* jobs;  // kJobs entries, ready flags zeroed before the launch
+  JobQueue* jobs;  // counters and kJobs entries, zeroed before the launch
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
@@ -530,11 +540,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   emit.next = &P.ctr->next;
   emit.chunk = P.chunk;
   emit.jobs = kShare ? P.jobs : nullptr;
-  emit.ctr = P.ctr;
   (void)warps;
   while (true) {
     // pieces of other windows' contained ranges first
-    const long long h = (kShare && P.jobs) ? take_job(P.ctr) : -1;
+    const long long h = (kShare && P.jobs) ? take_job(P.jobs) : -1;
     if (h >= 0) {
       run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
       continue;
@@ -542,7 +551,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     unsigned long long t = 0;
     if (lane_id() == 0) {
       t = atomicAdd(&P.ctr->ticket, 1ull);
-      if (kShare && (long long)t < nq) atomicAdd(&P.ctr->active, 1ull);
+      if (kShare && P.jobs && (long long)t < nq) atomicAdd(&P.jobs->active, 1ull);
     }
     t = __shfl_sync(0xffffffffu, t, 0);
     if ((long long)t >= nq) break;
@@ -551,25 +560,28 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     emit.begin(q);
     traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
              P.stack_cap, emit, &P.ctr->error);
-    if (kShare) {
+    if (kShare && P.jobs) {
       __syncwarp();
-      if (lane_id() == 0) atomicAdd(&P.ctr->active, ~0ull);  // -1
+      if (lane_id() == 0) atomicAdd(&P.jobs->active, ~0ull);  // -1
     }
   }
   // No windows left: while other warps are still inside windows, stay to take
   // the pieces they may publish.  Leaving is always safe (a finder drains its
   // own pieces), so the wait is bounded and ends without an error.
   if (kShare && P.jobs) {
-    for (uint32_t spin = 0; spin < kSpinLimit; spin++) {
-      const long long h = take_job(P.ctr);
+    uint32_t nap = 256;
+    for (uint32_t spin = 0; spin < kSpinLimit / 64; spin++) {
+      const long long h = take_job(P.jobs);
       if (h >= 0) {
         run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
+        nap = 256;
         continue;
       }
       int busy = 0;
-      if (lane_id() == 0) busy = ld_relaxed_ull(&P.ctr->active) != 0;
+      if (lane_id() == 0) busy = ld_relaxed_ull(&P.jobs->active) != 0;
       if (!__shfl_sync(0xffffffffu, busy, 0)) break;
-      __nanosleep(1000);
+      __nanosleep(nap);  // idle: poll less and less often, up to every 16 us
+      nap = min(2u * nap, 16384u);
     }
   }
   if (lane_id() == 0) {
@@ -858,7 +870,7 @@ struct PersistScratch {
   void* sort_zero;
   SortBufs bufs;
   long long max_holes;
-  RangeJob* jobs;
+  JobQueue* jobs;
   size_t bytes;
 };
 
@@ -866,7 +878,7 @@ static size_t persist_scratch_bytes(int64_t max_nq, long long max_holes, bool so
 {
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   size_t b = al(sizeof(QueryCounters)) + 2 * al(sizeof(Hole) * max_holes) +
-             al(sizeof(long long) * (max_holes + 1)) + al(sizeof(RangeJob) * kJobs);
+             al(sizeof(long long) * (max_holes + 1)) + al(kJobQueueBytes);
   if (sort) b += al(sort_zero_bytes(max_nq)) + 4 * al(4 * (size_t)std::max<int64_t>(max_nq, 1));
   return b;
 }
@@ -880,7 +892,7 @@ static void persist_scratch_carve(char* base, int64_t max_nq, long long max_hole
   S.holes = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
   S.sorted = (Hole*)(base + off); off += al(sizeof(Hole) * max_holes);
   S.cum = (long long*)(base + off); off += al(sizeof(long long) * (max_holes + 1));
-  S.jobs = (RangeJob*)(base + off); off += al(sizeof(RangeJob) * kJobs);
+  S.jobs = (JobQueue*)(base + off); off += al(kJobQueueBytes);
   S.sort_zero = nullptr;
   if (sort) {
     S.sort_zero = base + off; off += al(sort_zero_bytes(max_nq));
@@ -904,7 +916,7 @@ static void enqueue_pre(const WindowView& W, int64_t max_nq, const PersistScratc
 {
   // counters (keep nq), the job queue's ready flags and the sort's zeroed block
   cudaMemsetAsync(S.ctr, 0, offsetof(QueryCounters, nq), stream);
-  cudaMemsetAsync(S.jobs, 0, sizeof(RangeJob) * kJobs, stream);
+  cudaMemsetAsync(S.jobs, 0, kJobQueueBytes, stream);
   if (sort && max_nq > 0) {
     const int sms = sm_count();
     cudaMemsetAsync(S.sort_zero, 0, sort_zero_bytes(max_nq), stream);
