@@ -116,13 +116,13 @@ struct OffsetEmit {
 
 // ---------------------------------------------------------------------------
 // Range sharing (persistent form).  One window can own a contained subtree of
-// millions of boxes; copying it with one warp would leave the rest of the GPU
-// idle at the end of a batch.  The warp that finds such a range reserves its
-// output, cuts it into kPiece-id pieces, publishes them in a job queue and
-// goes on with its window.  Warps take pieces before each new window and
-// before they leave, and a warp leaves only when the queue is empty (or no
-// window is in progress any more), so every published piece is copied; a
-// taker waits, bounded, only for the few stores that publish its piece.
+// millions of boxes; copied by one warp it leaves the rest of the GPU idle at
+// the end of a batch.  The warp that finds such a range reserves its output,
+// cuts it into kPiece-id pieces, publishes them in a job queue and goes on
+// with its window.  Warps that find no window left claim queue indices with
+// one fetch-and-add each and copy the pieces as they are published, so the
+// tail of a batch runs on every warp of the GPU.  A claimed index that no
+// window will ever fill ends the claimer's wait once every window is done.
 // ---------------------------------------------------------------------------
 struct RangeJob {
   long long first;  // first sorted slot
@@ -132,15 +132,15 @@ struct RangeJob {
   unsigned ready;   // 1 once published; the taker clears it
   int pad;
 };
-// The queue's counters, each on its own 128-byte line: idle warps poll them,
-// and they must not share a line with the ticket and output counters every
-// busy warp updates.
+// The queue's counters, each on its own 128-byte line: waiting warps poll
+// them, and they must not share a line with the ticket and output counters
+// every busy warp updates.
 struct JobQueue {
   unsigned long long tail;  // pieces reserved
   unsigned long long pad0[15];
-  unsigned long long head;  // pieces taken
+  unsigned long long head;  // queue indices claimed
   unsigned long long pad1[15];
-  unsigned long long active;  // warps inside a window's traversal
+  unsigned long long active;  // warps holding (or taking) a window
   unsigned long long pad2[15];
   RangeJob entries[1];  // kJobs
 };
@@ -149,58 +149,42 @@ constexpr int kPiece = 16384;          // ids per piece
 constexpr int kShareMin = 2 * kPiece;  // ranges shorter than this stay with their finder
 constexpr size_t kJobQueueBytes = offsetof(JobQueue, entries) + sizeof(RangeJob) * kJobs;
 
-// Takes the next published-or-reserved piece; -1 when the queue is empty
-// (warp-collective).
-__device__ __forceinline__ long long take_job(JobQueue* Q)
-{
-  long long h = -1;
-  if (lane_id() == 0) {
-    for (int attempt = 0;; attempt++) {
-      const unsigned long long hh = ld_relaxed_ull(&Q->head);
-      const unsigned long long t = min(ld_relaxed_ull(&Q->tail), (unsigned long long)kJobs);
-      if (hh >= t) break;
-      if (atomicCAS(&Q->head, hh, hh + 1) == hh) {
-        h = (long long)hh;
-        break;
-      }
-      __nanosleep(32u << min(attempt, 5));  // lost the race: back off
-    }
-  }
-  return __shfl_sync(0xffffffffu, h, 0);
-}
+__device__ __forceinline__ void fence_sc_gpu() { asm volatile("fence.sc.gpu;" ::: "memory"); }
 
-// Copies piece `h` once its publisher has written it (warp-collective).
-__device__ __forceinline__ void run_job(JobQueue* Q, long long h, const int* bid,
-                                        int32_t* fid, int32_t* tid, long long cap, int* err)
+// Waits (lane 0) until queue index h is published, and takes the piece; 0 when
+// h will never be published (every window is done and h was not reserved) or
+// the bounded wait ran out (an error is recorded).
+__device__ __forceinline__ int wait_piece(JobQueue* Q, const QueryCounters* ctr,
+                                          unsigned long long nq, long long h, RangeJob& out,
+                                          int* err)
 {
   RangeJob* J = Q->entries + h;
-  long long first = 0, slot = 0;
-  int count = 0, q = 0, ok = 0;
-  if (lane_id() == 0) {
-    for (uint32_t spin = 0; spin < kSpinLimit; spin++) {
-      if (ld_acquire_u32(&J->ready)) {
-        ok = 1;
-        break;
-      }
-      if (spin > 32) __nanosleep(64);
-    }
-    if (ok) {
-      first = J->first;
-      slot = J->slot;
-      count = J->count;
-      q = J->q;
+  uint32_t nap = 64;
+  for (uint32_t spin = 0; spin < kSpinLimit / 16; spin++) {
+    if (ld_acquire_u32(&J->ready)) {
+      out.first = J->first;
+      out.slot = J->slot;
+      out.count = J->count;
+      out.q = J->q;
       J->ready = 0;
-    } else {
-      raise_error(err, CRT_ERR_DEVICE_TIMEOUT);
+      return 1;
     }
+    if (ld_relaxed_ull(&Q->tail) <= (unsigned long long)h) {
+      // not reserved yet: can any window still reserve it?
+      fence_sc_gpu();
+      const unsigned long long t = ld_relaxed_ull(&ctr->ticket);
+      fence_sc_gpu();
+      const unsigned long long a = ld_relaxed_ull(&Q->active);
+      if (t >= nq && a == 0) {
+        fence_sc_gpu();
+        if (ld_relaxed_ull(&Q->tail) <= (unsigned long long)h) return 0;
+      }
+    }
+    __nanosleep(nap);
+    nap = min(2u * nap, 8192u);
   }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (!ok) return;
-  first = __shfl_sync(0xffffffffu, first, 0);
-  slot = __shfl_sync(0xffffffffu, slot, 0);
-  count = __shfl_sync(0xffffffffu, count, 0);
-  q = __shfl_sync(0xffffffffu, q, 0);
-  copy_range(bid, first, count, fid, tid, slot, cap, q);
+  raise_error(err, CRT_ERR_DEVICE_TIMEOUT);
+  return 0;
 }
 
 // Warp-reserved output chunks (persistent form).
@@ -540,18 +524,19 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   emit.next = &P.ctr->next;
   emit.chunk = P.chunk;
   emit.jobs = kShare ? P.jobs : nullptr;
+  JobQueue* Q = kShare ? P.jobs : nullptr;
   (void)warps;
   while (true) {
-    // pieces of other windows' contained ranges first
-    const long long h = (kShare && P.jobs) ? take_job(P.jobs) : -1;
-    if (h >= 0) {
-      run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
-      continue;
-    }
     unsigned long long t = 0;
     if (lane_id() == 0) {
+      // a warp counts as active before it takes a ticket, so a waiting warp
+      // that sees the tickets gone and no warp active knows no window is left
+      if (Q) {
+        atomicAdd(&Q->active, 1ull);
+        fence_sc_gpu();
+      }
       t = atomicAdd(&P.ctr->ticket, 1ull);
-      if (kShare && P.jobs && (long long)t < nq) atomicAdd(&P.jobs->active, 1ull);
+      if (Q && (long long)t >= nq) atomicAdd(&Q->active, ~0ull);  // -1
     }
     t = __shfl_sync(0xffffffffu, t, 0);
     if ((long long)t >= nq) break;
@@ -560,28 +545,30 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     emit.begin(q);
     traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
              P.stack_cap, emit, &P.ctr->error);
-    if (kShare && P.jobs) {
+    if (Q) {
       __syncwarp();
-      if (lane_id() == 0) atomicAdd(&P.jobs->active, ~0ull);  // -1
+      if (lane_id() == 0) {
+        fence_sc_gpu();  // this window's reservations before it stops counting
+        atomicAdd(&Q->active, ~0ull);
+      }
     }
   }
-  // No windows left: while other warps are still inside windows, stay to take
-  // the pieces they may publish.  Leaving is always safe (a finder drains its
-  // own pieces), so the wait is bounded and ends without an error.
-  if (kShare && P.jobs) {
-    uint32_t nap = 256;
-    for (uint32_t spin = 0; spin < kSpinLimit / 64; spin++) {
-      const long long h = take_job(P.jobs);
-      if (h >= 0) {
-        run_job(P.jobs, h, P.T.bid, P.fid, P.tid, P.cap, &P.ctr->error);
-        nap = 256;
-        continue;
-      }
-      int busy = 0;
-      if (lane_id() == 0) busy = ld_relaxed_ull(&P.jobs->active) != 0;
-      if (!__shfl_sync(0xffffffffu, busy, 0)) break;
-      __nanosleep(nap);  // idle: poll less and less often, up to every 16 us
-      nap = min(2u * nap, 16384u);
+  // No window left: copy published pieces until no window can publish more.
+  if (Q) {
+    while (true) {
+      long long h = 0;
+      if (lane_id() == 0) h = (long long)atomicAdd(&Q->head, 1ull);
+      h = __shfl_sync(0xffffffffu, h, 0);
+      if (h >= kJobs) break;  // past the queue: never published
+      RangeJob J{};
+      int got = 0;
+      if (lane_id() == 0) got = wait_piece(Q, P.ctr, (unsigned long long)nq, h, J, &P.ctr->error);
+      if (!__shfl_sync(0xffffffffu, got, 0)) break;
+      const long long first = __shfl_sync(0xffffffffu, J.first, 0);
+      const long long slot = __shfl_sync(0xffffffffu, J.slot, 0);
+      const int count = __shfl_sync(0xffffffffu, J.count, 0);
+      const int jq = __shfl_sync(0xffffffffu, J.q, 0);
+      copy_range(P.T.bid, first, count, P.fid, P.tid, slot, P.cap, jq);
     }
   }
   if (lane_id() == 0) {
