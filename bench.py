@@ -71,6 +71,8 @@ def parse():
                    help="comma list of legs to skip: build,e2e,plain,cpu,serve,adversarial")
     p.add_argument("--adv-boxes", type=int, default=50_000_000)
     p.add_argument("--adv-windows", type=int, default=2_000_000)
+    p.add_argument("--adv-buffer-log2", type=int, default=32,
+                   help="output buffer of the streamed adversarial leg: 2^k pairs")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-rates", default="1000,10000",
@@ -543,9 +545,9 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     """Road-like boxes (centres on 100 segments, Pareto long sides capped at
     0.5, aspect ratios up to 1e4) and a window mix of 50% points, 40% small
     windows and 10% windows over 1% of the domain.  Batched: every window
-    through query_stream (one 2^30-pair output buffer reused, batches that
-    overflow re-run smaller); pairs are counted and dropped, as a consumer
-    that reduces them would.  Served: the first tenth of the windows as
+    through query_stream (one output buffer of 2^32 pairs, 32 GiB, reused;
+    batches that overflow re-run smaller); pairs are counted and dropped, as
+    a consumer that reduces them would.  Served: the first tenth of the windows as
     requests of 1-1000 windows arriving at 1k requests/s."""
     import time
 
@@ -561,7 +563,7 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     C.build_rtree(d, rt)
     dq = C.BBox.from_host(q)
     total = C.query_stats(rt, d, dq)["hits"]
-    cap = C.query_capacity(1 << 30)
+    cap = C.query_capacity(1 << args.adv_buffer_log2)
     drop = lambda f, t, a: None
     warm = C.BBox(dq.xmin[:20_000], dq.ymin[:20_000], dq.xmax[:20_000], dq.ymax[:20_000],
                   dq.id[:20_000])
