@@ -15,7 +15,7 @@ Headline (one JSON line on rank 0):
           copies the windows from pinned host memory, queries, and copies every
           hit pair back to pinned host memory.
   serving four resident trees (1M-50M boxes), 400 requests of 1-100k
-          windows arriving as a Poisson stream at 1k and 10k requests/s:
+          windows arriving as a Poisson stream at 1k, 3k and 10k requests/s:
           continuous batching against the plain form one request at a time,
           windows/s and p50/p99 latency.
   roofline  of the dominant kernel (the persistent traversal): algorithmic bytes
@@ -75,7 +75,7 @@ def parse():
                    help="output buffer of the streamed adversarial leg: 2^k pairs")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
     p.add_argument("--serve-requests", type=int, default=400)
-    p.add_argument("--serve-rates", default="1000,10000",
+    p.add_argument("--serve-rates", default="1000,3000,10000",
                    help="comma list of Poisson arrival rates (requests/s)")
     p.add_argument("--serve-max-batch", type=int, default=100_000)
     p.add_argument("--serve-arena-gb", type=int, default=64)
