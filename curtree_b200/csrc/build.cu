@@ -1,18 +1,19 @@
 // Z-order bulk load (replaces build_rtree, src/rtree_bulkload_thrust.cuh:62-213).
 //
 // Pipeline, all on one stream, no host synchronisation until the end:
-//   1. encode      read the box SoA once (float4 loads where aligned), write the
-//                  flipped 32-bit Morton key and a 32-byte AoS copy of each box
-//                  (one DRAM sector, so the later random gather costs one
-//                  sector per box), and count all four 8-bit key digits.
+//   1. encode      read the box SoA (float4 loads where aligned), write the
+//                  flipped 32-bit Morton key and the slot of a 32-byte AoS
+//                  record of each box (records of a 4096-box tile grouped by
+//                  the key's top digit), and count all four 8-bit key digits.
 //   2. plan        one CTA: which digit passes are non-uniform (a uniform digit
 //                  leaves a stable order unchanged, so its pass is skipped) and
 //                  the global bucket start of every digit value.
 //   3. 4 x onesweep  stable LSD radix passes over (key, slot) with decoupled
 //                  look-back across tiles: one read and one write of the pairs
-//                  per pass.  The first active pass makes the slot values, the
-//                  last one writes only slots.
-//   4. leaf level  gather each sorted box from the AoS copy, write the permuted
+//                  per pass.  The first active pass reads the encoder's slots,
+//                  the last one writes only slots.
+//   4. leaf level  gather each sorted box's record (runs of one top digit per
+//                  tile, so lines are shared by neighbouring records), write the permuted
 //                  SoA, and reduce every run of `fanout` boxes into its
 //                  leaf-parent node.
 //   5. upper levels  reduce runs of `fanout` nodes, level by level up to the root.
@@ -46,59 +47,165 @@ constexpr uint64_t kFlagIncl = 2ull << 62;
 // ---------------------------------------------------------------------------
 // 1. encode
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void encode_one(float a, float b, float c, float d, int id, int64_t i,
-                                           uint32_t* keys, Box32* aos, uint32_t (*sh)[kBins])
+// Each CTA takes tiles of kEncTile boxes.  Per box it writes the key and, in
+// input order, the slot of the box's 32-byte record; the records of a tile
+// are placed in its own slot range grouped by the key's top digit.  The sort
+// then carries those slots (its first pass reads them instead of making
+// input indices), and the leaf level's gather in sorted order, which walks
+// one top digit at a time, reads each tile's run for that digit (about
+// kEncTile / 256 records, often several whole 128-byte lines) instead of
+// single records scattered over the whole copy.  Order inside a run does not
+// matter: ties in the sort keep input order because the (key, slot) pairs
+// start in input order.
+constexpr int kEncThreads = 512;
+constexpr int kEncGroups = 2;                            // float4 groups per thread
+constexpr int kEncTile = 4 * kEncGroups * kEncThreads;   // 4096 boxes
+
+struct BoxIn {
+  const float* __restrict__ xmin;
+  const float* __restrict__ ymin;
+  const float* __restrict__ xmax;
+  const float* __restrict__ ymax;
+  const int* __restrict__ id;
+};
+
+// Loads boxes j..j+3 (those below n); kVec: the arrays are 16-byte aligned.
+template <bool kVec>
+__device__ __forceinline__ void load4(const BoxIn& in, int64_t j, int64_t n, float4& a, float4& b,
+                                      float4& c, float4& d, int4& e)
 {
-  uint32_t k = sort_key(a, b, c, d);
-  keys[i] = k;
-  Box32 bx;
-  bx.mbr = make_float4(a, b, c, d);
-  bx.idp = make_int4(id, 0, 0, 0);
-  aos[i] = bx;
-  atomicAdd(&sh[0][k & 0xFF], 1u);
-  atomicAdd(&sh[1][(k >> 8) & 0xFF], 1u);
-  atomicAdd(&sh[2][(k >> 16) & 0xFF], 1u);
-  atomicAdd(&sh[3][k >> 24], 1u);
+  if (kVec && j + 3 < n) {
+    a = reinterpret_cast<const float4*>(in.xmin)[j >> 2];
+    b = reinterpret_cast<const float4*>(in.ymin)[j >> 2];
+    c = reinterpret_cast<const float4*>(in.xmax)[j >> 2];
+    d = reinterpret_cast<const float4*>(in.ymax)[j >> 2];
+    e = reinterpret_cast<const int4*>(in.id)[j >> 2];
+    return;
+  }
+  float* pa = &a.x;
+  float* pb = &b.x;
+  float* pc = &c.x;
+  float* pd = &d.x;
+  int* pe = &e.x;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const bool v = j + k < n;
+    pa[k] = v ? in.xmin[j + k] : 0.f;
+    pb[k] = v ? in.ymin[j + k] : 0.f;
+    pc[k] = v ? in.xmax[j + k] : 0.f;
+    pd[k] = v ? in.ymax[j + k] : 0.f;
+    pe[k] = v ? in.id[j + k] : 0;
+  }
 }
 
 template <bool kVec>
-__global__ void __launch_bounds__(256) encode_kernel(const float* __restrict__ xmin,
-                                                     const float* __restrict__ ymin,
-                                                     const float* __restrict__ xmax,
-                                                     const float* __restrict__ ymax,
-                                                     const int* __restrict__ id, int64_t n,
-                                                     uint32_t* __restrict__ keys,
-                                                     Box32* __restrict__ aos,
-                                                     uint32_t* __restrict__ hist)
+__global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n,
+                                                             uint32_t* __restrict__ keys,
+                                                             uint32_t* __restrict__ slots,
+                                                             Box32* __restrict__ aos,
+                                                             uint32_t* __restrict__ hist)
 {
-  __shared__ uint32_t sh[4][kBins];
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
-  __syncthreads();
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  if (kVec) {
-    const int64_t n4 = n / 4;
-    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n4; g += stride) {
-      float4 a = reinterpret_cast<const float4*>(xmin)[g];
-      float4 b = reinterpret_cast<const float4*>(ymin)[g];
-      float4 c = reinterpret_cast<const float4*>(xmax)[g];
-      float4 d = reinterpret_cast<const float4*>(ymax)[g];
-      int4 e = reinterpret_cast<const int4*>(id)[g];
-      encode_one(a.x, b.x, c.x, d.x, e.x, 4 * g + 0, keys, aos, sh);
-      encode_one(a.y, b.y, c.y, d.y, e.y, 4 * g + 1, keys, aos, sh);
-      encode_one(a.z, b.z, c.z, d.z, e.z, 4 * g + 2, keys, aos, sh);
-      encode_one(a.w, b.w, c.w, d.w, e.w, 4 * g + 3, keys, aos, sh);
+  __shared__ uint32_t sh[3][kBins];  // digits 0..2 over all of this CTA's tiles
+  __shared__ uint32_t s_top[kBins];  // digit 3 over all of this CTA's tiles
+  __shared__ uint32_t s_run[kBins];  // this tile: count, then run start, per top digit
+  __shared__ uint32_t s_wsum[kBins / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < 3 * kBins; i += kEncThreads) (&sh[0][0])[i] = 0;
+  if (tid < kBins) s_top[tid] = 0;
+  const int64_t ntiles = (n + kEncTile - 1) / kEncTile;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if (tid < kBins) s_run[tid] = 0;
+    __syncthreads();
+    const int64_t base = t * kEncTile;
+    uint32_t key[4 * kEncGroups], rank[4 * kEncGroups];
+#pragma unroll
+    for (int g = 0; g < kEncGroups; g++) {
+      const int64_t j = base + 4 * (tid + g * kEncThreads);
+      float4 a, b, c, d;
+      int4 e;
+      load4<kVec>(in, j, n, a, b, c, d, e);
+      const float* pa = &a.x;
+      const float* pb = &b.x;
+      const float* pc = &c.x;
+      const float* pd = &d.x;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint32_t kk = sort_key(pa[k], pb[k], pc[k], pd[k]);
+        key[4 * g + k] = kk;
+        rank[4 * g + k] = 0;
+        if (j + k < n) {
+          rank[4 * g + k] = atomicAdd(&s_run[kk >> 24], 1u);
+          atomicAdd(&sh[0][kk & 0xFF], 1u);
+          atomicAdd(&sh[1][(kk >> 8) & 0xFF], 1u);
+          atomicAdd(&sh[2][(kk >> 16) & 0xFF], 1u);
+        }
+      }
+      if (j + 3 < n) {
+        *reinterpret_cast<uint4*>(keys + j) =
+            make_uint4(key[4 * g], key[4 * g + 1], key[4 * g + 2], key[4 * g + 3]);
+      } else {
+        for (int k = 0; k < 4; k++)
+          if (j + k < n) keys[j + k] = key[4 * g + k];
+      }
     }
-    for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-      encode_one(xmin[i], ymin[i], xmax[i], ymax[i], id[i], i, keys, aos, sh);
-  } else {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-      encode_one(xmin[i], ymin[i], xmax[i], ymax[i], id[i], i, keys, aos, sh);
+    __syncthreads();
+    // run starts: exclusive prefix of the tile's top-digit counts
+    uint32_t cnt = 0, x = 0;
+    if (tid < kBins) {
+      cnt = s_run[tid];
+      s_top[tid] += cnt;
+      x = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) s_wsum[warp] = x;
+    }
+    __syncthreads();
+    if (tid < kBins) {
+      uint32_t start = x - cnt;
+      for (int w = 0; w < warp; w++) start += s_wsum[w];
+      s_run[tid] = start;
+    }
+    __syncthreads();
+    // records into their runs; slots in input order
+#pragma unroll
+    for (int g = 0; g < kEncGroups; g++) {
+      const int64_t j = base + 4 * (tid + g * kEncThreads);
+      float4 a, b, c, d;
+      int4 e;
+      load4<kVec>(in, j, n, a, b, c, d, e);  // second read of the tile: from L2
+      const float* pa = &a.x;
+      const float* pb = &b.x;
+      const float* pc = &c.x;
+      const float* pd = &d.x;
+      const int* pe = &e.x;
+      uint32_t sl[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        sl[k] = (uint32_t)base + s_run[key[4 * g + k] >> 24] + rank[4 * g + k];
+        if (j + k < n) {
+          Box32 bx;
+          bx.mbr = make_float4(pa[k], pb[k], pc[k], pd[k]);
+          bx.idp = make_int4(pe[k], 0, 0, 0);
+          aos[sl[k]] = bx;
+        }
+      }
+      if (j + 3 < n) {
+        *reinterpret_cast<uint4*>(slots + j) = make_uint4(sl[0], sl[1], sl[2], sl[3]);
+      } else {
+        for (int k = 0; k < 4; k++)
+          if (j + k < n) slots[j + k] = sl[k];
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) {
-    uint32_t v = (&sh[0][0])[i];
+  for (int i = tid; i < 3 * kBins; i += kEncThreads) {
+    const uint32_t v = (&sh[0][0])[i];
     if (v) atomicAdd(&hist[i], v);
   }
+  if (tid < kBins && s_top[tid]) atomicAdd(&hist[3 * kBins + tid], s_top[tid]);
 }
 
 // ---------------------------------------------------------------------------
@@ -373,8 +480,9 @@ __global__ void __launch_bounds__(kLevelThreads)
   const int64_t c1 = min(nchild, p1 * fanout);
   const uint32_t* sorted = nullptr;
   if (kLeaf) {
+    // record slots in sorted order (the encoder's slots when no pass ran)
     int na = ctrl->n_active;
-    sorted = na == 0 ? nullptr : ((na & 1) ? vals1 : vals0);
+    sorted = (na & 1) ? vals1 : vals0;
   }
   // this thread's parent (if any) and its child range
   const int64_t my = p0 + threadIdx.x;
@@ -393,7 +501,7 @@ __global__ void __launch_bounds__(kLevelThreads)
 #pragma unroll
       for (int u = 0; u < kGather; u++) {
         const int64_t s = cb + threadIdx.x + u * kLevelThreads;
-        src[u] = s < ce ? (sorted ? (int64_t)sorted[s] : s) : 0;
+        src[u] = s < ce ? (int64_t)sorted[s] : 0;
         if (src[u] >= nchild) src[u] = s < ce ? s : 0;  // only after a sort error (reported)
       }
       Box32 bx[kGather];
@@ -539,20 +647,20 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
     const int sms = sm_count();
     const bool vec = aligned16(in_xmin) && aligned16(in_ymin) && aligned16(in_xmax) &&
                      aligned16(in_ymax) && aligned16(in_id);
-    int64_t work = vec ? cdiv(n, 4) : n;
-    int grid = (int)std::min<int64_t>(cdiv(work, 256), (int64_t)sms * 8);
+    int grid = (int)std::min<int64_t>(cdiv(n, kEncTile), (int64_t)sms * 2);
     if (grid < 1) grid = 1;
+    const BoxIn bin{in_xmin, in_ymin, in_xmax, in_ymax, in_id};
     {
     ProfScope ps("encode", stream);
     if (vec)
-      encode_kernel<true><<<grid, 256, 0, stream>>>(in_xmin, in_ymin, in_xmax, in_ymax, in_id, n,
-                                                    bufs.keys[0], aos, hist);
+      encode_kernel<true><<<grid, kEncThreads, 0, stream>>>(bin, n, bufs.keys[0], bufs.vals[0],
+                                                            aos, hist);
     else
-      encode_kernel<false><<<grid, 256, 0, stream>>>(in_xmin, in_ymin, in_xmax, in_ymax, in_id,
-                                                     n, bufs.keys[0], aos, hist);
+      encode_kernel<false><<<grid, kEncThreads, 0, stream>>>(bin, n, bufs.keys[0], bufs.vals[0],
+                                                             aos, hist);
     }
     CRT_LAUNCHED(1);
-    sort_passes(bufs, n, scratch, stream);
+    sort_passes(bufs, n, scratch, stream, kSortGivenValues);
 
     // leaf-parent level
     int64_t parent_start = rsz;
