@@ -57,8 +57,8 @@ constexpr uint64_t kFlagIncl = 2ull << 62;
 // single records scattered over the whole copy.  Order inside a run does not
 // matter: ties in the sort keep input order because the (key, slot) pairs
 // start in input order.
-constexpr int kEncThreads = 512;
-constexpr int kEncGroups = 2;                            // float4 groups per thread
+constexpr int kEncThreads = 256;
+constexpr int kEncGroups = 4;                            // float4 groups per thread
 constexpr int kEncTile = 4 * kEncGroups * kEncThreads;   // 4096 boxes
 
 struct BoxIn {
@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
   __shared__ uint32_t s_top[kBins];  // digit 3 over all of this CTA's tiles
   __shared__ uint32_t s_run[kBins];  // this tile: count, then run start, per top digit
   __shared__ uint32_t s_wsum[kBins / 32];
+  __shared__ uint32_t s_dr[kEncTile];  // per box of the tile: top digit << 16 | rank in its run
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int i = tid; i < 3 * kBins; i += kEncThreads) (&sh[0][0])[i] = 0;
   if (tid < kBins) s_top[tid] = 0;
@@ -117,10 +118,10 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
     if (tid < kBins) s_run[tid] = 0;
     __syncthreads();
     const int64_t base = t * kEncTile;
-    uint32_t key[4 * kEncGroups], rank[4 * kEncGroups];
 #pragma unroll
     for (int g = 0; g < kEncGroups; g++) {
-      const int64_t j = base + 4 * (tid + g * kEncThreads);
+      const int i0 = 4 * (tid + g * kEncThreads);  // first box of the group in the tile
+      const int64_t j = base + i0;
       float4 a, b, c, d;
       int4 e;
       load4<kVec>(in, j, n, a, b, c, d, e);
@@ -128,24 +129,23 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
       const float* pb = &b.x;
       const float* pc = &c.x;
       const float* pd = &d.x;
+      uint32_t kk[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        const uint32_t kk = sort_key(pa[k], pb[k], pc[k], pd[k]);
-        key[4 * g + k] = kk;
-        rank[4 * g + k] = 0;
+        kk[k] = sort_key(pa[k], pb[k], pc[k], pd[k]);
         if (j + k < n) {
-          rank[4 * g + k] = atomicAdd(&s_run[kk >> 24], 1u);
-          atomicAdd(&sh[0][kk & 0xFF], 1u);
-          atomicAdd(&sh[1][(kk >> 8) & 0xFF], 1u);
-          atomicAdd(&sh[2][(kk >> 16) & 0xFF], 1u);
+          const uint32_t top = kk[k] >> 24;
+          s_dr[i0 + k] = top << 16 | atomicAdd(&s_run[top], 1u);
+          atomicAdd(&sh[0][kk[k] & 0xFF], 1u);
+          atomicAdd(&sh[1][(kk[k] >> 8) & 0xFF], 1u);
+          atomicAdd(&sh[2][(kk[k] >> 16) & 0xFF], 1u);
         }
       }
       if (j + 3 < n) {
-        *reinterpret_cast<uint4*>(keys + j) =
-            make_uint4(key[4 * g], key[4 * g + 1], key[4 * g + 2], key[4 * g + 3]);
+        *reinterpret_cast<uint4*>(keys + j) = make_uint4(kk[0], kk[1], kk[2], kk[3]);
       } else {
         for (int k = 0; k < 4; k++)
-          if (j + k < n) keys[j + k] = key[4 * g + k];
+          if (j + k < n) keys[j + k] = kk[k];
       }
     }
     __syncthreads();
@@ -172,7 +172,8 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
     // records into their runs; slots in input order
 #pragma unroll
     for (int g = 0; g < kEncGroups; g++) {
-      const int64_t j = base + 4 * (tid + g * kEncThreads);
+      const int i0 = 4 * (tid + g * kEncThreads);
+      const int64_t j = base + i0;
       float4 a, b, c, d;
       int4 e;
       load4<kVec>(in, j, n, a, b, c, d, e);  // second read of the tile: from L2
@@ -184,7 +185,8 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
       uint32_t sl[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        sl[k] = (uint32_t)base + s_run[key[4 * g + k] >> 24] + rank[4 * g + k];
+        const uint32_t dr = j + k < n ? s_dr[i0 + k] : 0u;
+        sl[k] = (uint32_t)base + s_run[dr >> 16] + (dr & 0xFFFFu);
         if (j + k < n) {
           Box32 bx;
           bx.mbr = make_float4(pa[k], pb[k], pc[k], pd[k]);
@@ -495,14 +497,14 @@ __global__ void __launch_bounds__(kLevelThreads)
     const int64_t ce = min(c1, cb + (int64_t)kLevelChunk);
     if (kLeaf) {
       // all slot loads, then all 32-byte record loads, then the stores: each
-      // thread keeps kGather random sector reads in flight
+      // thread keeps kGather record reads in flight
       constexpr int kGather = kLevelChunk / kLevelThreads;
-      int64_t src[kGather];
+      uint32_t src[kGather];
 #pragma unroll
       for (int u = 0; u < kGather; u++) {
         const int64_t s = cb + threadIdx.x + u * kLevelThreads;
-        src[u] = s < ce ? (int64_t)sorted[s] : 0;
-        if (src[u] >= nchild) src[u] = s < ce ? s : 0;  // only after a sort error (reported)
+        src[u] = s < ce ? sorted[s] : 0u;
+        if ((int64_t)src[u] >= nchild) src[u] = s < ce ? (uint32_t)s : 0u;  // only after a sort error (reported)
       }
       Box32 bx[kGather];
 #pragma unroll
@@ -647,7 +649,7 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
     const int sms = sm_count();
     const bool vec = aligned16(in_xmin) && aligned16(in_ymin) && aligned16(in_xmax) &&
                      aligned16(in_ymax) && aligned16(in_id);
-    int grid = (int)std::min<int64_t>(cdiv(n, kEncTile), (int64_t)sms * 2);
+    int grid = (int)std::min<int64_t>(cdiv(n, kEncTile), (int64_t)sms * 3);
     if (grid < 1) grid = 1;
     const BoxIn bin{in_xmin, in_ymin, in_xmax, in_ymax, in_id};
     {
