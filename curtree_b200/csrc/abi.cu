@@ -3,6 +3,8 @@
 // query pipelines.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -77,6 +79,16 @@ static bool tree_ok(const crt_rtree_f32* t)
 // one's output before its exact count is known.
 static std::atomic<double> g_pairs_per_window{64.0};
 
+// The drop-in query runs into a working buffer from the stream-ordered pool
+// (sized from the last call's pairs per window, re-run once at the exact size
+// if that was too small), then copies the pairs into exact-size cudaMalloc
+// arrays, which the caller frees with cudaFree as the reference's
+// idpair_d_free does (src/utility.cuh:164-195).  Batches below
+// kDropinPersistentMin windows take the plain form: its fixed cost (no
+// window sort, no chunk compaction) is far below the persistent form's,
+// which wins on large batches.
+constexpr int64_t kDropinPersistentMin = 32768;
+
 static int query_dropin(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                         const crt_bbox_f32* d_qbox, crt_idpair* d_dq, cudaStream_t stream)
 {
@@ -85,22 +97,27 @@ static int query_dropin(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   init_device();
   crt_query_opts o;
   crt_query_opts_default(&o);
-  crt_query_result* res = nullptr;
-  CRT_CUDA(cudaMalloc((void**)&res, sizeof(crt_query_result)));
   const int64_t nq = d_qbox->sz;
+  if (nq < kDropinPersistentMin) o.mode = CRT_QUERY_PLAIN;
   int64_t want = (int64_t)(g_pairs_per_window.load() * (double)nq * 1.25) + 1024;
+  crt_query_result* res = nullptr;
+  if (cudaMallocAsync((void**)&res, sizeof(crt_query_result), stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRT_ERR_OOM, "query: result block allocation failed");
+  }
   int rc = CRT_OK;
-  int32_t *fid = nullptr, *tid = nullptr;
+  int32_t* work = nullptr;
+  int64_t cap = 0;
   crt_query_result h{};
   for (int attempt = 0; attempt < 3; attempt++) {
-    const int64_t cap = query_capacity(want, o);
-    if (cudaMalloc((void**)&fid, sizeof(int32_t) * (size_t)cap) != cudaSuccess ||
-        cudaMalloc((void**)&tid, sizeof(int32_t) * (size_t)cap) != cudaSuccess) {
+    cap = query_capacity(want, o);
+    if (cudaMallocAsync((void**)&work, 2 * sizeof(int32_t) * (size_t)cap, stream) != cudaSuccess) {
       cudaGetLastError();
+      work = nullptr;
       rc = fail(CRT_ERR_OOM, "query: output allocation failed");
       break;
     }
-    rc = query_into(*d_rt, *d_rbox, *d_qbox, fid, tid, cap, res, nullptr, o, stream);
+    rc = query_into(*d_rt, *d_rbox, *d_qbox, work, work + cap, cap, res, nullptr, o, stream);
     if (rc != CRT_OK) break;
     cudaError_t e = cudaMemcpyAsync(&h, res, sizeof(h), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -113,15 +130,29 @@ static int query_dropin(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
       break;
     }
     if (!h.overflow) break;
-    cudaFree(fid);
-    cudaFree(tid);
-    fid = tid = nullptr;
+    cudaFreeAsync(work, stream);
+    work = nullptr;
     want = h.required;  // exact: the retry cannot overflow
   }
-  cudaFree(res);
   if (rc == CRT_OK && h.overflow) rc = fail(CRT_ERR_CUDA, "query: output overflow after retry");
   if (rc == CRT_OK && h.count > INT32_MAX)
     rc = fail(CRT_ERR_OVERFLOW_INT32, "query: more than INT32_MAX pairs; use crt_query_into_f32");
+  int32_t *fid = nullptr, *tid = nullptr;
+  if (rc == CRT_OK) {
+    const size_t bytes = sizeof(int32_t) * (size_t)std::max<int64_t>(h.count, 1);
+    if (cudaMalloc((void**)&fid, bytes) != cudaSuccess || cudaMalloc((void**)&tid, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      rc = fail(CRT_ERR_OOM, "query: output allocation failed");
+    } else if (h.count > 0) {
+      cudaMemcpyAsync(fid, work, sizeof(int32_t) * (size_t)h.count, cudaMemcpyDeviceToDevice, stream);
+      cudaMemcpyAsync(tid, work + cap, sizeof(int32_t) * (size_t)h.count, cudaMemcpyDeviceToDevice,
+                      stream);
+    }
+  }
+  if (work) cudaFreeAsync(work, stream);
+  cudaFreeAsync(res, stream);
+  cudaError_t e = cudaStreamSynchronize(stream);
+  if (rc == CRT_OK && e != cudaSuccess) rc = cuda_fail(e, "query: copy");
   if (rc != CRT_OK) {
     if (fid) cudaFree(fid);
     if (tid) cudaFree(tid);

@@ -585,18 +585,29 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   }
 }
 
-// Sorts the recorded holes by start (rank by counting: the list is short).
-__global__ void hole_sort_kernel(const Hole* __restrict__ holes, Hole* __restrict__ sorted,
-                                 const QueryCounters* __restrict__ ctr, long long max_holes)
+// Sorts the recorded holes by start: rank by counting (starts are distinct:
+// holes do not overlap), one hole per thread, all starts streamed through
+// shared memory in tiles.
+constexpr int kHoleTile = 2048;
+
+__global__ void __launch_bounds__(256)
+    hole_sort_kernel(const Hole* __restrict__ holes, Hole* __restrict__ sorted,
+                     const QueryCounters* __restrict__ ctr, long long max_holes)
 {
+  __shared__ long long s_start[kHoleTile];
   const long long nh = min((long long)ctr->nholes, max_holes);
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nh;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long s = holes[i].start;
-    long long r = 0;
-    for (long long j = 0; j < nh; j++) r += holes[j].start < s;
-    sorted[r] = holes[i];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((long long)blockIdx.x * blockDim.x >= nh) return;  // whole CTA idle
+  const long long my = i < nh ? holes[i].start : 0;
+  long long r = 0;
+  for (long long t0 = 0; t0 < nh; t0 += kHoleTile) {
+    const int m = (int)min((long long)kHoleTile, nh - t0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < m; k += blockDim.x) s_start[k] = holes[t0 + k].start;
+    __syncthreads();
+    for (int k = 0; k < m; k++) r += s_start[k] < my;
   }
+  if (i < nh) sorted[r] = holes[i];
 }
 
 // Exclusive prefix of the sorted hole lengths (one CTA).
@@ -636,12 +647,30 @@ __device__ __forceinline__ long long holes_below(const Hole* h, const long long*
   return cum[i] + min(x - h[i].start, h[i].len);
 }
 
-// Moves every pair stored at or above `hits` into the holes below it, so the
-// output is dense [0, hits); then writes the result block.
-__global__ void compact_kernel(const Hole* __restrict__ h, const long long* __restrict__ cum,
-                               QueryCounters* __restrict__ ctr, long long max_holes,
-                               int32_t* fid, int32_t* tid, long long cap,
-                               crt_query_result* __restrict__ res)
+// First hole (sorted by start) whose start is >= x.
+__device__ __forceinline__ long long hole_at_or_after(const Hole* h, long long nh, long long x)
+{
+  long long lo = 0, hi = nh;
+  while (lo < hi) {
+    long long m = (lo + hi) >> 1;
+    if (h[m].start < x) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// Moves every pair stored at or above `hits` (T) into the holes below it, so
+// the output is dense [0, T); then writes the result block.  The B pairs to
+// move are the data slots of [T, next) in order, and their destinations the
+// hole slots below T in order: both are runs, so each CTA takes a piece of
+// kMovePiece consecutive moves, finds where its sources and destinations
+// start with binary searches, and then copies run by run with coalesced
+// accesses.
+constexpr long long kMovePiece = 8192;
+
+__global__ void __launch_bounds__(256)
+    compact_kernel(const Hole* __restrict__ h, const long long* __restrict__ cum,
+                   QueryCounters* __restrict__ ctr, long long max_holes, int32_t* fid,
+                   int32_t* tid, long long cap, crt_query_result* __restrict__ res)
 {
   const long long nh = min((long long)ctr->nholes, max_holes);
   const long long T = (long long)ctr->hits;
@@ -654,27 +683,59 @@ __global__ void compact_kernel(const Hole* __restrict__ h, const long long* __re
     res->error = ctr->error;
   }
   if (overflow || ctr->error || nh == 0) return;
-  const long long below_T = holes_below(h, cum, nh, T);
-  for (long long s = T + (long long)blockIdx.x * blockDim.x + threadIdx.x; s < R;
-       s += (long long)gridDim.x * blockDim.x) {
-    // inside a hole?
-    long long lo = 0, hi = nh;
-    while (lo < hi) {
-      long long m = (lo + hi) >> 1;
-      if (h[m].start <= s) lo = m + 1; else hi = m;
+  const long long B = holes_below(h, cum, nh, T);  // pairs to move
+  for (long long r0 = (long long)blockIdx.x * kMovePiece; r0 < B;
+       r0 += (long long)gridDim.x * kMovePiece) {
+    long long rem = min(kMovePiece, B - r0);
+    // destination of move r0: the r0-th hole slot below T
+    long long a = 0;
+    {
+      long long lo = 0, hi = nh;  // last hole with cum <= r0
+      while (hi - lo > 1) {
+        const long long m = (lo + hi) >> 1;
+        if (cum[m] <= r0) lo = m; else hi = m;
+      }
+      a = lo;
     }
-    if (lo > 0 && s < h[lo - 1].start + h[lo - 1].len) continue;
-    const long long r = (s - T) - (holes_below(h, cum, nh, s) - below_T);
-    // r-th hole slot below T: last hole with cum <= r
-    long long a = 0, b = nh;
-    while (b - a > 1) {
-      long long m = (a + b) >> 1;
-      if (cum[m] <= r) a = m; else b = m;
+    long long d = h[a].start + (r0 - cum[a]);
+    // source of move r0: the smallest x >= T with r0 + 1 data slots in [T, x]
+    long long s = T;
+    {
+      long long lo = T, hi = R - 1;
+      while (lo < hi) {
+        const long long m = (lo + hi) >> 1;
+        const long long data = (m + 1 - T) - (holes_below(h, cum, nh, m + 1) - B);
+        if (data >= r0 + 1) hi = m; else lo = m + 1;
+      }
+      s = lo;
     }
-    const long long dst = h[a].start + (r - cum[a]);
-    if (dst < T && dst >= 0) {
-      fid[dst] = fid[s];
-      tid[dst] = tid[s];
+    long long jn = hole_at_or_after(h, nh, s + 1);  // next hole above the source
+    while (rem > 0) {
+      const long long src_end = jn < nh ? h[jn].start : R;
+      const long long dst_end = min(h[a].start + h[a].len, T);
+      const long long n = min(rem, min(src_end - s, dst_end - d));
+      if (n <= 0 || d < 0 || s + n > R || d + n > T) {  // inconsistent holes: report, stop
+        if (threadIdx.x == 0) raise_error(&res->error, CRT_ERR_CUDA);
+        break;
+      }
+      for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        fid[d + i] = fid[s + i];
+        tid[d + i] = tid[s + i];
+      }
+      s += n;
+      d += n;
+      rem -= n;
+      while (jn < nh && s == h[jn].start) {  // skip the hole(s) above the source
+        s = h[jn].start + h[jn].len;
+        jn++;
+      }
+      if (rem > 0 && d == dst_end) {
+        if (++a >= nh) {
+          if (threadIdx.x == 0) raise_error(&res->error, CRT_ERR_CUDA);
+          break;
+        }
+        d = h[a].start;
+      }
     }
   }
 }
