@@ -140,7 +140,7 @@ struct JobQueue {
   unsigned long long pad0[15];
   unsigned long long head;  // queue indices claimed
   unsigned long long pad1[15];
-  unsigned long long active;  // warps holding (or taking) a window
+  unsigned long long active;  // warps not yet past their ticket loop
   unsigned long long pad2[15];
   RangeJob entries[1];  // kJobs
 };
@@ -526,18 +526,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
   emit.jobs = kShare ? P.jobs : nullptr;
   JobQueue* Q = kShare ? P.jobs : nullptr;
   (void)warps;
+  // a warp counts as active from before its first ticket until it has left
+  // the ticket loop, so a waiting warp that sees the tickets gone and no
+  // warp active knows no window can publish any more
+  if (Q && lane_id() == 0) {
+    atomicAdd(&Q->active, 1ull);
+    fence_sc_gpu();
+  }
   while (true) {
     unsigned long long t = 0;
-    if (lane_id() == 0) {
-      // a warp counts as active before it takes a ticket, so a waiting warp
-      // that sees the tickets gone and no warp active knows no window is left
-      if (Q) {
-        atomicAdd(&Q->active, 1ull);
-        fence_sc_gpu();
-      }
-      t = atomicAdd(&P.ctr->ticket, 1ull);
-      if (Q && (long long)t >= nq) atomicAdd(&Q->active, ~0ull);  // -1
-    }
+    if (lane_id() == 0) t = atomicAdd(&P.ctr->ticket, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
     if ((long long)t >= nq) break;
     int q = order ? (int)order[t] : (int)t;
@@ -545,12 +543,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     emit.begin(q);
     traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
              P.stack_cap, emit, &P.ctr->error);
-    if (Q) {
-      __syncwarp();
-      if (lane_id() == 0) {
-        fence_sc_gpu();  // this window's reservations before it stops counting
-        atomicAdd(&Q->active, ~0ull);
-      }
+  }
+  if (Q) {
+    __syncwarp();
+    if (lane_id() == 0) {
+      fence_sc_gpu();  // this warp's reservations before it stops counting
+      atomicAdd(&Q->active, ~0ull);  // -1
     }
   }
   // No window left: copy published pieces until no window can publish more.

@@ -98,7 +98,7 @@ struct SrvState {
   long long r_start;  // oldest request a fresh warp may meet
   int shutdown;
   int error;
-  unsigned long long windows_done;
+  unsigned long long reserved;
 };
 
 constexpr int kSrvThreads = 256;
@@ -255,7 +255,6 @@ __global__ void __launch_bounds__(kSrvThreads)
     if (lane == 0) {
       __threadfence();
       const unsigned long long fin = atomicAdd(&ctr->done, 1ull) + 1;
-      atomicAdd(&st->windows_done, 1ull);
       if ((long long)fin == d.nq) {
         __threadfence();
         const unsigned long long count = ld_volatile_u64(&ctr->next);
