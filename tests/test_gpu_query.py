@@ -280,3 +280,33 @@ def test_query_stats_match_oracle(crt):
     assert st["tested"] == int(want.tested.sum())
     assert 0 <= st["tested_contain"] <= st["tested"]
     assert 0 <= st["range_hits"] <= st["hits"]
+
+
+def test_query_stream_edges(crt):
+    """Streamed batches: an empty window set gives no batch and no pairs; a
+    window whose own pairs exceed the buffer is CRT_ERR_OUTPUT_OVERFLOW; a
+    buffer below the form's chunk slack is rejected."""
+    b = D.uniform_boxes(200_000, seed=91)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(16)
+    crt.build_rtree(d, rt)
+    got = []
+    empty = crt.BBox.empty(0)
+    st = crt.query_stream(rt, d, empty, lambda f, t, a: got.append(f.numel()),
+                          capacity=1 << 20, mode=crt.CRT_QUERY_PLAIN)
+    assert st == {"pairs": 0, "batches": 0, "retries": 0} and not got
+    # one window over the whole domain: 200k pairs against a 1000-pair buffer
+    big = HostBoxes(np.array([-1.0], np.float32), np.array([-1.0], np.float32),
+                      np.array([1e9], np.float32), np.array([1e9], np.float32),
+                      np.array([0], np.int32))
+    dq = crt.BBox.from_host(big)
+    with pytest.raises(crt.CrtError):
+        crt.query_stream(rt, d, dq, lambda *a: None, capacity=1000, mode=crt.CRT_QUERY_PLAIN)
+    with pytest.raises(crt.CrtError):
+        crt.query_stream(rt, d, dq, lambda *a: None, capacity=1000)
+    # the same window with room: every box once
+    ids = []
+    st = crt.query_stream(rt, d, dq, lambda f, t, a: ids.append(f.cpu().numpy()),
+                          capacity=1 << 20, mode=crt.CRT_QUERY_PLAIN)
+    assert st["pairs"] == b.n
+    assert np.array_equal(np.sort(np.concatenate(ids)), np.arange(b.n, dtype=np.int32))
