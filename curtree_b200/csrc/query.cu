@@ -102,8 +102,8 @@ struct OffsetEmit {
     if (!m) return;
     long long slot = base + __popc(m & lanemask_lt());
     if (hit && slot < cap) {
-      fid[slot] = id;
-      tid[slot] = q;
+      __stcs(fid + slot, id);
+      __stcs(tid + slot, q);
     }
     base += __popc(m);
   }
@@ -221,8 +221,8 @@ struct ChunkEmit {
       end = (long long)nb + chunk;
     }
     if (hit && slot < cap) {
-      fid[slot] = id;
-      tid[slot] = q;
+      __stcs(fid + slot, id);
+      __stcs(tid + slot, q);
     }
   }
   // A contained subtree's ids are copied to an exact reservation of their
