@@ -443,8 +443,10 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     const uint2 kv = s_kv[j];
     const int dst = s_gbase[digit_of(kv.x, shift)] + j;
     if ((uint32_t)dst < (uint32_t)n) {
-      if (!last) dst_k[dst] = kv.x;
-      dst_v[dst] = kv.y;
+      // evict-first: a pass's output is read once, by the next pass, and
+      // the look-back status words and the next tiles' runs want L2
+      if (!last) __stcs(dst_k + dst, kv.x);
+      __stcs(dst_v + dst, kv.y);
     }
   }
 }
@@ -515,11 +517,11 @@ __global__ void __launch_bounds__(kLevelThreads)
         const int64_t s = cb + threadIdx.x + u * kLevelThreads;
         if (s < ce) {
           const float4 m = bx[u].mbr;
-          oxmin[s] = m.x;
-          oymin[s] = m.y;
-          oxmax[s] = m.z;
-          oymax[s] = m.w;
-          oid[s] = bx[u].idp.x;
+          __stcs(oxmin + s, m.x);
+          __stcs(oymin + s, m.y);
+          __stcs(oxmax + s, m.z);
+          __stcs(oymax + s, m.w);
+          __stcs(oid + s, bx[u].idp.x);
           s_mbr[s - cb] = m;
         }
       }
