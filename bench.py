@@ -12,8 +12,10 @@ Headline (one JSON line on rank 0):
           log-normal sides, 1% duplicates, 1% points): encode + radix sort +
           node build, boxes/s.
   e2e     the same query metric through the C ABI with host buffers: each step
-          copies the windows from pinned host memory, queries, and copies every
-          hit pair back to pinned host memory.
+          copies the windows from pinned host memory, queries, reads the pair
+          count and copies every result back to pinned host memory (as CSR:
+          ids + offsets, or as pairs; the faster is reported, with the other
+          beside it).
   serving four resident trees (1M-50M boxes), 400 requests of 1-100k
           windows arriving as a Poisson stream at 1k, 3k and 10k requests/s:
           continuous batching against the plain form one request at a time,
@@ -374,45 +376,76 @@ def run_ours(args, rank, world, dist):
 
 
 def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, dist, world):
-    """Windows H2D from pinned host memory, query, all pairs D2H to pinned host
-    memory, per step, through the C ABI."""
+    """End to end through the C ABI with host buffers, per step: the windows
+    H2D from pinned host memory, the query, the result block D2H (the pair
+    count), then every result D2H to pinned host memory.  Two result forms:
+    CSR (plain form: box ids grouped by window + int64 offsets, 4 B per pair)
+    and pairs (persistent form: box id + window index, 8 B per pair).  The
+    faster is the headline e2e; both are reported."""
     import psutil
     import torch
     nwin = windows.n
-    pair_bytes = 8 * pairs
-    # every rank on this node pins its own pair buffers: budget a share each
+    # every rank on this node pins its own result buffers: budget a share each
     local = max(1, int(os.environ.get("LOCAL_WORLD_SIZE", "1")))
     avail = psutil.virtual_memory().available / local
-    if pair_bytes * 1.5 > avail:
+    if 8 * pairs * 1.5 > avail:
         return {"value": None, "unit": "windows/s",
-                "skipped": f"host memory share {avail / 1e9:.0f} GB < 1.5 x {pair_bytes / 1e9:.0f} GB of pairs"}
+                "skipped": f"host memory share {avail / 1e9:.0f} GB < 1.5 x {8 * pairs / 1e9:.0f} GB of pairs"}
     h_win = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
              for a in (windows.xmin, windows.ymin, windows.xmax, windows.ymax, windows.id)]
-    h_fid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
-    h_tid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
+    h2d = sum(int(h.numel() * h.element_size()) for h in h_win)
     d_win = C.BBox.empty(nwin)
     dst = [d_win.xmin, d_win.ymin, d_win.xmax, d_win.ymax, d_win.id]
     h_res = torch.empty(64, dtype=torch.uint8, pin_memory=True)
+    offs = torch.empty(nwin + 1, dtype=torch.int64, device="cuda")
+    h_fid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
 
-    def step():
+    def run(step, d2h_per_step, path):
+        for _ in range(max(1, min(args.warmup, 2))):
+            step()
+        torch.cuda.synchronize()
+        r = C.read_result(h_res)
+        assert r["count"] == pairs and r["overflow"] == 0, r
+        ms = reduce_max(timed(step, args.steps, stream), dist)
+        return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h_per_step,
+                "ms_per_step": ms / args.steps, "path": path}
+
+    def h2d_windows():
         for d, h in zip(dst, h_win):
             d.copy_(h, non_blocking=True)
-        C.query_into(rt, sorted_box, d_win, fid, tid, res)
-        h_res.copy_(res, non_blocking=True)
-        h_fid.copy_(fid[:pairs], non_blocking=True)
-        h_tid.copy_(tid[:pairs], non_blocking=True)
 
-    for _ in range(max(1, min(args.warmup, 2))):
-        step()
-    torch.cuda.synchronize()
-    r = C.read_result(h_res)
-    assert r["count"] == pairs and r["overflow"] == 0, r
-    ms = timed(step, args.steps, stream)
-    ms = reduce_max(ms, dist)
-    h2d = sum(int(h.numel() * h.element_size()) for h in h_win)
-    return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
-            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8 * pairs + 64,
-            "ms_per_step": ms / args.steps, "path": "crt_query_into_f32 (persistent) via ctypes"}
+    def count():
+        h_res.copy_(res, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return C.read_result(h_res)["count"]
+
+    # CSR: box ids grouped by window and the offsets
+    h_offs = torch.empty(nwin + 1, dtype=torch.int64, pin_memory=True)
+
+    def step_csr():
+        h2d_windows()
+        C.query_into(rt, sorted_box, d_win, fid, None, res, offs, C.CRT_QUERY_PLAIN)
+        n = count()
+        h_offs.copy_(offs, non_blocking=True)
+        h_fid[:n].copy_(fid[:n], non_blocking=True)
+
+    csr = run(step_csr, 4 * pairs + 8 * (nwin + 1) + 64,
+              "crt_query_into_f32 (plain form, CSR: ids + offsets) via ctypes")
+    del h_offs
+    # pairs: box id and window index
+    h_tid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
+
+    def step_pairs():
+        h2d_windows()
+        C.query_into(rt, sorted_box, d_win, fid, tid, res)
+        n = count()
+        h_fid[:n].copy_(fid[:n], non_blocking=True)
+        h_tid[:n].copy_(tid[:n], non_blocking=True)
+
+    prs = run(step_pairs, 8 * pairs + 64, "crt_query_into_f32 (persistent form, pairs) via ctypes")
+    best, other = (csr, prs) if csr["value"] >= prs["value"] else (prs, csr)
+    return dict(best, alternative=other)
 
 
 def serving_workload(args, rank):

@@ -331,6 +331,9 @@ int crt_query_into_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   crt_query_opts o;
   crt_query_opts_default(&o);
   if (opts) o = *opts;
+  if (capacity > 0 && !d_fid) return fail(CRT_ERR_INVALID_ARG, "query_into: no id output");
+  if (capacity > 0 && !d_tid && (o.mode != CRT_QUERY_PLAIN || !d_offsets))
+    return fail(CRT_ERR_INVALID_ARG, "query_into: a window column is needed unless PLAIN writes offsets");
   return query_into(*d_rt, *d_rbox, *d_qbox, d_fid, d_tid, capacity, d_result, d_offsets, o,
                     (cudaStream_t)stream);
 }

@@ -103,7 +103,7 @@ struct OffsetEmit {
     long long slot = base + __popc(m & lanemask_lt());
     if (hit && slot < cap) {
       __stcs(fid + slot, id);
-      __stcs(tid + slot, q);
+      if (tid) __stcs(tid + slot, q);  // no window column: CSR output
     }
     base += __popc(m);
   }
@@ -1058,7 +1058,10 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   if (qbox.sz < 0 || rbox.sz < 0 || rt.sz < 0)
     return fail(CRT_ERR_INVALID_ARG, "query: negative size");
   if (rt.sz > 0 && rt.fanout < 2) return fail(CRT_ERR_INVALID_ARG, "query: fanout < 2");
-  if (capacity > 0 && (!fid || !tid)) return fail(CRT_ERR_INVALID_ARG, "query: null output");
+  if (capacity > 0 && !fid) return fail(CRT_ERR_INVALID_ARG, "query: null output");
+  // without a window column the output is CSR: only the plain form with offsets
+  if (capacity > 0 && !tid && (opts.mode != CRT_QUERY_PLAIN || !d_offsets))
+    return fail(CRT_ERR_INVALID_ARG, "query: null window column outside PLAIN with offsets");
   TreeView T = make_view(rt, rbox);
   const LevelTables lt = opts.no_contain ? LevelTables() : level_tables(rt, rbox.sz);
   WindowView W{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, qbox.sz};

@@ -142,7 +142,7 @@ __device__ __forceinline__ void put_pair(int32_t* __restrict__ fid, int32_t* __r
 {
   if (slot < cap) {
     __stcs(fid + slot, id);
-    __stcs(tid + slot, q);
+    if (tid) __stcs(tid + slot, q);  // no window column: CSR output
   }
 }
 
@@ -172,9 +172,10 @@ __device__ __forceinline__ void copy_range(const int* __restrict__ bid, long lon
       const long long g = g0 + u * 32 + lane;
       if (g < nv) {
         const long long sl = s + 4 * g;
-        if (sl + 3 < cap && ((((uintptr_t)(fid + sl)) | ((uintptr_t)(tid + sl))) & 15) == 0) {
+        const uintptr_t al = (uintptr_t)(fid + sl) | (tid ? (uintptr_t)(tid + sl) : (uintptr_t)0);
+        if (sl + 3 < cap && (al & 15) == 0) {
           __stcs(reinterpret_cast<int4*>(fid + sl), r[u]);
-          __stcs(reinterpret_cast<int4*>(tid + sl), make_int4(q, q, q, q));
+          if (tid) __stcs(reinterpret_cast<int4*>(tid + sl), make_int4(q, q, q, q));
         } else {
           put_pair(fid, tid, sl + 0, cap, r[u].x, q);
           put_pair(fid, tid, sl + 1, cap, r[u].y, q);

@@ -230,13 +230,16 @@ def query_into(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, fid, tid, result, offset
                mode: int = _lib.CRT_QUERY_PERSISTENT, stream=None, **opts) -> None:
     """Asynchronous extended query into caller-owned torch tensors: fid/tid
     (int32, capacity = numel), result (uint8 x 64 on the device, the
-    crt_query_result block), offsets (int64, nq + 1, plain mode only)."""
+    crt_query_result block), offsets (int64, nq + 1, plain mode only).  In
+    plain mode with offsets, tid may be None: the output is then CSR (box
+    ids of window w at fid[offsets[w]:offsets[w + 1]])."""
     o = _lib.default_opts(mode=mode, **opts)
     rb, qb = d_rbox.c(), d_qbox.c()
     cap = int(fid.numel())
     check(load().crt_query_into_f32(ctypes.byref(d_rt.s), ctypes.byref(rb), ctypes.byref(qb),
                                     fid.data_ptr() if cap else None,
-                                    tid.data_ptr() if cap else None, cap, result.data_ptr(),
+                                    tid.data_ptr() if (cap and tid is not None) else None, cap,
+                                    result.data_ptr(),
                                     offsets.data_ptr() if offsets is not None else None,
                                     ctypes.byref(o), _stream_handle(stream)), "query_into")
 

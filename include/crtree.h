@@ -175,7 +175,9 @@ typedef struct {
  * pair count: grow the output to crt_query_capacity(required, ...) and call
  * again (overflow-and-retry).  PLAIN mode also writes per-window hit counts
  * (int64, nq + 1 entries, exclusive prefix) into d_offsets when non-NULL, and
- * its pairs come grouped by window in window order. */
+ * its pairs come grouped by window in window order.  PLAIN mode with
+ * d_offsets may pass d_tid = NULL: the result is then CSR (box ids of window
+ * w at d_fid[d_offsets[w] .. d_offsets[w + 1])), half the bytes of pairs. */
 int crt_query_into_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                        const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
                        int64_t capacity, crt_query_result* d_result, int64_t* d_offsets,

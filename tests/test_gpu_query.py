@@ -310,3 +310,37 @@ def test_query_stream_edges(crt):
                           capacity=1 << 20, mode=crt.CRT_QUERY_PLAIN)
     assert st["pairs"] == b.n
     assert np.array_equal(np.sort(np.concatenate(ids)), np.arange(b.n, dtype=np.int32))
+
+
+def test_plain_csr_without_window_column(crt):
+    """Plain form with offsets and no window column: the box ids and offsets
+    equal those of the pair output, and the window of every id follows from
+    the offsets (CSR).  Without offsets, or in the persistent form, a missing
+    window column is rejected."""
+    import torch
+    b = D.uniform_boxes(300_000, seed=95)
+    q = D.mixed_windows(5_000, b, seed=195)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(16)
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    fid, tid, offs = crt.query(rt, d, dq, mode=crt.CRT_QUERY_PLAIN)
+    n = fid.numel()
+    fid2 = torch.empty(n, dtype=torch.int32, device="cuda")
+    offs2 = torch.empty(q.n + 1, dtype=torch.int64, device="cuda")
+    res = crt.new_result_block()
+    crt.query_into(rt, d, dq, fid2, None, res, offs2, crt.CRT_QUERY_PLAIN)
+    r = crt.read_result(res)
+    assert r["count"] == n and not r["overflow"] and not r["error"]
+    assert torch.equal(offs2, offs) and torch.equal(fid2, fid)
+    counts = (offs2[1:] - offs2[:-1]).cpu().numpy()
+    tid_from_csr = np.repeat(np.arange(q.n, dtype=np.int32), counts)
+    assert np.array_equal(tid_from_csr, tid.cpu().numpy())
+    sb, t = O.build(b, 16)
+    want = canon(*O.tree_query_pairs(t, sb, q))
+    got = canon(fid2.cpu().numpy(), tid_from_csr)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    with pytest.raises(crt.CrtError):
+        crt.query_into(rt, d, dq, fid2, None, res, None, crt.CRT_QUERY_PLAIN)
+    with pytest.raises(crt.CrtError):
+        crt.query_into(rt, d, dq, fid2, None, res, offs2, crt.CRT_QUERY_PERSISTENT)
