@@ -189,6 +189,10 @@ def make_query_inputs(rank: int, nbox: int, nwin: int):
     return boxes, windows
 
 
+# A serving replay that has not finished by then is a fault, not a slow run.
+SERVE_DEADLINE_S = 120.0
+
+
 def traffic_for(kernel: str, units: float):
     """DRAM bytes per launch of `kernel` from the committed ncu summary
     (profiles/traffic.json: bytes measured on a smaller launch and the units
@@ -478,6 +482,8 @@ def serve_run(srv, tids, reqs, arrivals):
     t0 = time.monotonic()
     while done < len(reqs):
         now = time.monotonic() - t0
+        if now > SERVE_DEADLINE_S:
+            raise RuntimeError(f"serving run passed {SERVE_DEADLINE_S} s: {done} of {len(reqs)} done")
         while nxt < len(reqs) and arrivals[nxt] <= now:
             backlog.append(nxt)
             nxt += 1
@@ -634,6 +640,8 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     t0 = time.monotonic()
     while done < len(reqs):
         now = time.monotonic() - t0
+        if now > SERVE_DEADLINE_S:
+            raise RuntimeError(f"serving run passed {SERVE_DEADLINE_S} s: {done} of {len(reqs)} done")
         while nxt < len(reqs) and arrivals[nxt] <= now:
             backlog.append(nxt)
             nxt += 1

@@ -785,11 +785,32 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
     const bool host_windows = cudaPointerGetAttributes(&pa, xmin) == cudaSuccess &&
                               pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged;
     cudaGetLastError();
-    q.predicted = host_windows ? s->predict_locked(tree_id, xmin, ymin, xmax, ymax, nq) : 0;
-    const double est = q.predicted > 0
-                           ? s->tree_stats[tree_id].corr * q.predicted * s->opts.output_slack + 256.0
-                           : s->tree_ppw[tree_id] * (double)nq * s->opts.output_slack + 256.0;
-    q.cap = (long long)std::min(est, 4.0e12);
+    if (host_windows) {
+      q.predicted = s->predict_locked(tree_id, xmin, ymin, xmax, ymax, nq);
+    } else {
+      // device-resident windows: the same area estimate from a host copy
+      // (16 B per window); a running pairs-per-window average is no guide
+      // when window sizes span orders of magnitude
+      std::vector<float> hw((size_t)nq * 4);
+      const float* src[4] = {xmin, ymin, xmax, ymax};
+      cudaError_t ce = cudaSuccess;
+      for (int a = 0; a < 4 && ce == cudaSuccess; a++)
+        ce = cudaMemcpy(hw.data() + (size_t)a * nq, src[a], sizeof(float) * (size_t)nq,
+                        cudaMemcpyDeviceToHost);
+      if (ce == cudaSuccess)
+        q.predicted = s->predict_locked(tree_id, hw.data(), hw.data() + nq, hw.data() + 2 * nq,
+                                        hw.data() + 3 * nq, nq);
+      else
+        cudaGetLastError();
+    }
+    double est = q.predicted > 0
+                     ? s->tree_stats[tree_id].corr * q.predicted * s->opts.output_slack + 256.0
+                     : s->tree_ppw[tree_id] * (double)nq * s->opts.output_slack + 256.0;
+    // no single estimate may hold more than a sixteenth of the arena: a
+    // request that needs more re-runs at its exact size (overflow-and-retry)
+    // instead of keeping everything behind it out of an arena it cannot fit
+    est = std::min(est, (double)s->arena_bytes / 16.0 / 8.0);
+    q.cap = (long long)std::max(256.0, std::min(est, 4.0e12));
     q.out_bytes = (size_t)q.cap * 8;
     if (!s->alloc.alloc(q.win_bytes, q.win_off))
       return fail(CRT_ERR_BUSY, "server_submit: arena full (windows)");
