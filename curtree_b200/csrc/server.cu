@@ -131,8 +131,8 @@ struct StagedEmit {
       for (int i = lane; i < n; i += 32) {
         const long long slot = (long long)b + i;
         if (slot < cap) {
-          __stcs(fid + slot, s_fid[i]);
-          __stcs(tid + slot, s_tid[i]);
+          fid[slot] = s_fid[i];
+          tid[slot] = s_tid[i];
         }
       }
       n = 0;
