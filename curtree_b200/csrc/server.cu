@@ -806,10 +806,10 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
     double est = q.predicted > 0
                      ? s->tree_stats[tree_id].corr * q.predicted * s->opts.output_slack + 256.0
                      : s->tree_ppw[tree_id] * (double)nq * s->opts.output_slack + 256.0;
-    // no single estimate may hold more than a sixteenth of the arena: a
-    // request that needs more re-runs at its exact size (overflow-and-retry)
-    // instead of keeping everything behind it out of an arena it cannot fit
-    est = std::min(est, (double)s->arena_bytes / 16.0 / 8.0);
+    // no single estimate may hold more than a quarter of the arena: an
+    // estimate past the arena would never be admitted, and a request that
+    // needs more re-runs at its exact size (overflow-and-retry)
+    est = std::min(est, (double)s->arena_bytes / 4.0 / 8.0);
     q.cap = (long long)std::max(256.0, std::min(est, 4.0e12));
     q.out_bytes = (size_t)q.cap * 8;
     if (!s->alloc.alloc(q.win_bytes, q.win_off))
