@@ -424,19 +424,64 @@ def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, d
         torch.cuda.current_stream().synchronize()
         return C.read_result(h_res)["count"]
 
-    # CSR: box ids grouped by window and the offsets
-    h_offs = torch.empty(nwin + 1, dtype=torch.int64, pin_memory=True)
+    # CSR: box ids grouped by window and the offsets, two steps in flight:
+    # step i's results cross PCIe while step i + 1 queries on the other
+    # stream (each step still copies its windows in and all its results out)
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    sets = []
+    for k in range(2):
+        with torch.cuda.stream(streams[k]):
+            w = C.BBox.empty(nwin)
+            f = fid if k == 0 else torch.empty(pairs, dtype=torch.int32, device="cuda")
+            sets.append({"win": w, "dst": [w.xmin, w.ymin, w.xmax, w.ymax, w.id], "fid": f,
+                         "offs": torch.empty(nwin + 1, dtype=torch.int64, device="cuda"),
+                         "res": C.new_result_block(),
+                         "h_res": torch.empty(64, dtype=torch.uint8, pin_memory=True),
+                         "h_fid": h_fid if k == 0 else torch.empty(pairs, dtype=torch.int32,
+                                                                    pin_memory=True),
+                         "h_offs": torch.empty(nwin + 1, dtype=torch.int64, pin_memory=True)})
+    torch.cuda.synchronize()
+    counter = [0]
 
     def step_csr():
-        h2d_windows()
-        C.query_into(rt, sorted_box, d_win, fid, None, res, offs, C.CRT_QUERY_PLAIN)
-        n = count()
-        h_offs.copy_(offs, non_blocking=True)
-        h_fid[:n].copy_(fid[:n], non_blocking=True)
+        k = counter[0] % 2
+        counter[0] += 1
+        st, z = streams[k], sets[k]
+        with torch.cuda.stream(st):
+            for d, h in zip(z["dst"], h_win):
+                d.copy_(h, non_blocking=True)
+            C.query_into(rt, sorted_box, z["win"], z["fid"], None, z["res"], z["offs"],
+                         C.CRT_QUERY_PLAIN, st)
+            z["h_res"].copy_(z["res"], non_blocking=True)
+            st.synchronize()  # the pair count sizes the copy out
+            n = C.read_result(z["h_res"])["count"]
+            z["h_offs"].copy_(z["offs"], non_blocking=True)
+            z["h_fid"][:n].copy_(z["fid"][:n], non_blocking=True)
 
-    csr = run(step_csr, 4 * pairs + 8 * (nwin + 1) + 64,
-              "crt_query_into_f32 (plain form, CSR: ids + offsets) via ctypes")
-    del h_offs
+    def run_csr():
+        for _ in range(max(1, min(args.warmup, 2))):
+            step_csr()
+        torch.cuda.synchronize()
+        r = C.read_result(sets[0]["h_res"])
+        assert r["count"] == pairs and r["overflow"] == 0, r
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_csr()
+        for st in streams:  # the last steps' copies out belong to the timed region
+            stream.wait_stream(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = reduce_max(e0.elapsed_time(e1), dist)
+        return {"value": world * nwin / (ms / args.steps / 1e3), "unit": "windows/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4 * pairs + 8 * (nwin + 1) + 64,
+                "ms_per_step": ms / args.steps,
+                "path": "crt_query_into_f32 (plain form, CSR: ids + offsets) via ctypes, "
+                        "two steps in flight on two streams"}
+
+    csr = run_csr()
+    del sets, streams
     # pairs: box id and window index
     h_tid = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
 
