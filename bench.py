@@ -75,6 +75,8 @@ def parse():
     p.add_argument("--adv-windows", type=int, default=2_000_000)
     p.add_argument("--adv-buffer-log2", type=int, default=32,
                    help="output buffer of the streamed adversarial leg: 2^k pairs")
+    p.add_argument("--ingest-records", type=int, default=4_000_000,
+                   help="records of the MBR text file the ingest leg reads")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-rates", default="1000,3000,10000",
@@ -371,6 +373,11 @@ def run_ours(args, rank, world, dist):
     # ---- adversarial geometry ------------------------------------------------------
     if "adversarial" not in skip:
         out["adversarial"] = adversarial_leg(args, C, stream, dist, world, rank)
+        torch.cuda.empty_cache()
+
+    # ---- ingest: MBR text file -> device boxes ---------------------------------
+    if "ingest" not in skip and rank == 0:
+        out["ingest"] = ingest_leg(args, C, L, stream)
         torch.cuda.empty_cache()
 
     # ---- bulk load ------------------------------------------------------------
@@ -722,6 +729,112 @@ def adversarial_leg(args, C, stream, dist, world, rank):
             "batched": batched, "served": served}
 
 
+def ingest_leg(args, C, L, stream):
+    """The reference's MBR text file read into device boxes: readMBR + box_h2d
+    (src/utility.cpp:5-40, src/utility.cuh:42-66) against
+    crt_read_mbr_csv_device, file in the page cache.  Each step is one call,
+    timed on the host clock (the call returns once the boxes are on the
+    device).  Beside it: the library's host loader (crt_read_mbr_csv, all
+    host threads) followed by the copy to the device, and a pinned
+    host-to-device copy of the same bytes, the link the device path rides."""
+    import ctypes
+    import tempfile
+    import time
+
+    import torch
+    from curtree_b200 import _lib
+    from curtree_b200 import datasets as D
+    n = args.ingest_records
+    boxes = D.uniform_boxes(n, seed=21)
+    boxes.id[:] = np.random.default_rng(22).integers(-2**31, 2**31 - 1, n)
+    text = D.mbr_csv_text(boxes)
+    nbytes = len(text)
+    shm = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    fd, path = tempfile.mkstemp(suffix=".csv", dir=shm)
+    try:
+        with os.fdopen(fd, "wb") as f:
+            f.write(text)
+        del text
+        box = _lib.crt_bbox_f32()
+        got = ctypes.c_int64(0)
+        h = ctypes.c_void_p(stream.cuda_stream)
+
+        def step():
+            t0 = time.perf_counter()
+            _lib.check(L.crt_read_mbr_csv_device(path.encode(), n, 0.0, ctypes.byref(box),
+                                                 ctypes.byref(got), h), "read_mbr_csv_device")
+            dt = time.perf_counter() - t0
+            return dt
+
+        L.crt_profile_enable(1)
+        for _ in range(args.warmup):
+            step()
+            L.crt_bbox_free(ctypes.byref(box))
+        profile_collect(None)
+        launches0 = C.kernel_launches()
+        secs = []
+        for i in range(args.steps):
+            secs.append(step())
+            if i + 1 < args.steps:
+                L.crt_bbox_free(ctypes.byref(box))
+        launches = C.kernel_launches() - launches0
+        parts = {k: profile_collect(k)[0] / args.steps
+                 for k in ("ingest_stage", "ingest_lines", "ingest_emit", "ingest_parse")}
+        profile_collect(None)
+        L.crt_profile_enable(0)
+        from curtree_b200.rtree import _d2h
+        dev = [_d2h(p, n, np.float32) for p in (box.xmin, box.ymin, box.xmax, box.ymax)]
+        dev_id = _d2h(box.id, n, np.int32)
+        L.crt_bbox_free(ctypes.byref(box))
+
+        # the host loader, then the copy of its arrays to the device
+        host = [np.empty(n, np.float32) for _ in range(4)]
+        host_id = np.empty(n, np.int32)
+        hsecs = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            _lib.check(L.crt_read_mbr_csv(path.encode(), n, 0.0, *[a.ctypes.data for a in host],
+                                          host_id.ctypes.data, ctypes.byref(got)), "read_mbr_csv")
+            d = [torch.from_numpy(a).cuda() for a in host + [host_id]]
+            torch.cuda.synchronize()
+            hsecs.append(time.perf_counter() - t0)
+            del d
+        identical = all(np.array_equal(a.view(np.uint32), b.view(np.uint32))
+                        for a, b in zip(host, dev)) and np.array_equal(host_id, dev_id)
+
+        # pinned host-to-device copy of the same number of bytes
+        src = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+        dst = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        for _ in range(2):
+            dst.copy_(src, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        h2d_gbs = 5 * nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9
+        del src, dst
+    finally:
+        os.unlink(path)
+    sec = statistics.median(secs)
+    kern_ms = parts["ingest_lines"] + parts["ingest_emit"] + parts["ingest_parse"]
+    return {"metric": "mbr_records_per_s", "value": n / sec, "unit": "records/s",
+            "text_gb_per_s": nbytes / sec / 1e9, "ms_per_step": sec * 1e3,
+            "records": n, "text_bytes": nbytes, "bytes_per_record": nbytes / n,
+            "phases_ms": parts, "gpu_kernels_ms": kern_ms,
+            "gpu_text_gb_per_s": nbytes / (kern_ms / 1e3) / 1e9 if kern_ms else None,
+            "gpu_launches": launches,
+            "h2d_pinned_gb_per_s": h2d_gbs, "frac_of_h2d_copy": nbytes / sec / 1e9 / h2d_gbs,
+            "host_loader": {"records_per_s": n / min(hsecs), "ms": min(hsecs) * 1e3,
+                            "cores": os.cpu_count(),
+                            "what": "crt_read_mbr_csv (host threads) + copy of the five arrays"},
+            "speedup_vs_host_loader": min(hsecs) / sec, "identical_to_host_loader": bool(identical),
+            "workload": f"{n // 10**6}M records 'x1,y1,x2,y2,id,pid,nume' (6 fraction digits, "
+                        "corners half swapped, random int32 ids), file in the page cache, "
+                        "crt_read_mbr_csv_device(path, n, r=0)"}
+
+
 def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
     import torch
     from curtree_b200 import datasets as D
@@ -826,6 +939,7 @@ def main():
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
                 "plain": out.get("plain"), "build": out.get("build"),
                 "serving": out.get("serving"), "adversarial": out.get("adversarial"),
+                "ingest": out.get("ingest"),
                 "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                 "persistent_kernel_ms": p["kernel_ms"]}
         if "plain" in out:

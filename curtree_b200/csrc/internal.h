@@ -60,4 +60,12 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
                int64_t* d_offsets, const crt_query_opts& opts, cudaStream_t stream);
 int64_t query_capacity(int64_t pairs, const crt_query_opts& opts);
 
+// Host parser of the reference's MBR text format (io.cu): one record at p
+// (false if malformed), the box readMBR makes of its four numbers, and the
+// whole loader over text in memory (statuses and *n_read as crt_read_mbr_csv).
+bool parse_mbr_record(const char* p, const char* end, float v[4], int& id);
+void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, float* ymax);
+int read_mbr_text(const char* base, size_t len, int64_t n, float r, float* xmin, float* ymin,
+                  float* xmax, float* ymax, int32_t* id, int64_t* n_read);
+
 }  // namespace crt

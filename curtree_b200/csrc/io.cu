@@ -57,8 +57,10 @@ inline const char* skip_ws(const char* p, const char* end)
   return p;
 }
 
+}  // namespace
+
 // One record "x1,y1,x2,y2,id,pid,nume" starting at p; false if malformed.
-bool parse_record(const char* p, const char* end, float v[4], int& id)
+bool parse_mbr_record(const char* p, const char* end, float v[4], int& id)
 {
   char buf[64];
   for (int f = 0; f < 7; f++) {
@@ -90,36 +92,30 @@ bool parse_record(const char* p, const char* end, float v[4], int& id)
   return true;
 }
 
-}  // namespace
-
-}  // namespace crt
-
-using namespace crt;
-
-extern "C" {
-
-int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* ymin, float* xmax,
-                     float* ymax, int32_t* id, int64_t* n_read)
+void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, float* ymax)
 {
-  if (!path || n < 0 || (n > 0 && !(xmin && ymin && xmax && ymax && id)))
-    return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv: bad arguments");
-  if (n_read) *n_read = 0;
-  std::string text;
-  if (!read_file(path, text)) return fail(CRT_ERR_INVALID_ARG, std::string("read_mbr_csv: cannot open ") + path);
+  // readMBR: min/max of the endpoints, then -/+ r (fp32)
+  *xmin = std::min(v[0], v[2]) - r;
+  *ymin = std::min(v[1], v[3]) - r;
+  *xmax = std::max(v[0], v[2]) + r;
+  *ymax = std::max(v[1], v[3]) + r;
+}
+
+int read_mbr_text(const char* base, size_t L, int64_t n, float r, float* xmin, float* ymin,
+                  float* xmax, float* ymax, int32_t* id, int64_t* n_read)
+{
   // record starts: non-empty lines
   std::vector<size_t> starts;
   starts.reserve((size_t)n);
   size_t i = 0;
-  const size_t L = text.size();
   while (i < L && (int64_t)starts.size() < n) {
     size_t j = i;
-    while (j < L && (text[j] == ' ' || text[j] == '\t' || text[j] == '\r')) j++;
-    if (j < L && text[j] != '\n') starts.push_back(j);
-    while (i < L && text[i] != '\n') i++;
+    while (j < L && (base[j] == ' ' || base[j] == '\t' || base[j] == '\r')) j++;
+    if (j < L && base[j] != '\n') starts.push_back(j);
+    while (i < L && base[i] != '\n') i++;
     i++;
   }
   const int64_t m = (int64_t)starts.size();
-  const char* base = text.data();
   const char* end = base + L;
   int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::vector<int64_t> bad(nt, -1);
@@ -130,15 +126,11 @@ int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* y
       for (int64_t k = t * per; k < std::min(m, (t + 1) * per); k++) {
         float v[4];
         int rid = 0;
-        if (!parse_record(base + starts[k], end, v, rid)) {
+        if (!parse_mbr_record(base + starts[k], end, v, rid)) {
           bad[t] = k;
           return;
         }
-        // readMBR: min/max of the endpoints, then -/+ r (fp32)
-        xmin[k] = std::min(v[0], v[2]) - r;
-        ymin[k] = std::min(v[1], v[3]) - r;
-        xmax[k] = std::max(v[0], v[2]) + r;
-        ymax[k] = std::max(v[1], v[3]) + r;
+        mbr_box(v, r, &xmin[k], &ymin[k], &xmax[k], &ymax[k]);
         id[k] = rid;
       }
     });
@@ -157,6 +149,23 @@ int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* y
     return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv: file holds " + std::to_string(m) +
                                          " records, " + std::to_string(n) + " requested");
   return CRT_OK;
+}
+
+}  // namespace crt
+
+using namespace crt;
+
+extern "C" {
+
+int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* ymin, float* xmax,
+                     float* ymax, int32_t* id, int64_t* n_read)
+{
+  if (!path || n < 0 || (n > 0 && !(xmin && ymin && xmax && ymax && id)))
+    return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv: bad arguments");
+  if (n_read) *n_read = 0;
+  std::string text;
+  if (!read_file(path, text)) return fail(CRT_ERR_INVALID_ARG, std::string("read_mbr_csv: cannot open ") + path);
+  return read_mbr_text(text.data(), text.size(), n, r, xmin, ymin, xmax, ymax, id, n_read);
 }
 
 int crt_bbox_free(crt_bbox_f32* b)

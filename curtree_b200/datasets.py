@@ -242,3 +242,62 @@ def serving_requests(n_requests: int, n_trees: int, seed: int = 104,
     size = np.exp(rng.uniform(np.log(lo), np.log(hi + 1), n_requests)).astype(np.int64)
     size = np.clip(size, lo, hi)
     return tree, size
+
+
+def _digit_count(a: np.ndarray) -> np.ndarray:
+    nd = np.ones(a.shape, np.int8)
+    for k in range(1, 19):
+        nd += a >= 10 ** k
+    return nd
+
+
+def mbr_csv_text(boxes: HostBoxes, decimals: int = 6, seed: int = 106) -> bytes:
+    """The boxes as the reference's MBR text records "x1,y1,x2,y2,id,pid,nume",
+    one per line (the format readMBR reads, src/utility.cpp:5-40): corners
+    printed with `decimals` fraction digits, the corners of half of the
+    records given in the opposite order (readMBR takes min/max of the
+    endpoints), pid in [0, 100), nume in [0, 10).  Vectorised numpy: the
+    records are laid out in a fixed-width byte matrix (numbers right-aligned,
+    NUL padding) whose padding is then squeezed out."""
+    rng = np.random.default_rng(seed)
+    n = boxes.n
+    swap = rng.random(n) < 0.5
+    f64 = lambda a: np.asarray(a, np.float64)
+    fields = [np.where(swap, f64(boxes.xmax), f64(boxes.xmin)),
+              np.where(swap, f64(boxes.ymax), f64(boxes.ymin)),
+              np.where(swap, f64(boxes.xmin), f64(boxes.xmax)),
+              np.where(swap, f64(boxes.ymin), f64(boxes.ymax)),
+              np.asarray(boxes.id, np.int64), rng.integers(0, 100, n), rng.integers(0, 10, n)]
+    scale = 10 ** decimals
+    parts = []  # (neg, integer part, its digit count, its widest count, fraction or None)
+    for k, v in enumerate(fields):
+        neg = v < 0
+        if k < 4:
+            q = np.rint(np.abs(v) * scale).astype(np.int64)
+            ip, fp = q // scale, q % scale
+        else:
+            ip, fp = np.abs(v).astype(np.int64), None
+        nd = _digit_count(ip)
+        parts.append((neg, ip, nd, int(nd.max(initial=1)), fp))
+    width = sum(1 + w + (1 + decimals if fp is not None else 0) + 1 for _, _, _, w, fp in parts)
+    M = np.zeros((width, n), np.uint8)  # column-major while writing, rows at the end
+    c = 0
+    for k, (neg, ip, nd, w, fp) in enumerate(parts):
+        # column c: room for the sign; digits right-aligned in c+1 .. c+w
+        x = ip
+        for j in range(w):
+            x, d = np.divmod(x, 10)
+            M[c + w - j] = np.where(nd > j, 48 + d, 0)
+        M[c + w - nd[neg], np.flatnonzero(neg)] = ord("-")
+        c += 1 + w
+        if fp is not None:
+            M[c] = ord(".")
+            x = fp
+            for j in range(decimals):
+                x, d = np.divmod(x, 10)
+                M[c + decimals - j] = 48 + d
+            c += 1 + decimals
+        M[c] = ord(",") if k < 6 else ord("\n")
+        c += 1
+    flat = np.ascontiguousarray(M.T).ravel()
+    return flat[flat != 0].tobytes()

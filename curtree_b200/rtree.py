@@ -387,5 +387,28 @@ class Plan:
             pass
 
 
+def read_mbr_csv(path: str, n: int = -1, r: float = 0.0, stream=None) -> BBox:
+    """readMBR (src/utility.cpp:5-40) followed by box_h2d
+    (src/utility.cuh:42-66), on the GPU: the records "x1,y1,x2,y2,id,pid,nume"
+    of the file become the device box set [min(x1,x2) - r, max(x1,x2) + r] x
+    [min(y1,y2) - r, max(y1,y2) + r] with the fifth field as id.  n = -1 reads
+    every record; otherwise exactly n records must be present.  A malformed
+    record or a short file raises CrtError (the reference exits or throws)."""
+    L = load()
+    box = _lib.crt_bbox_f32()
+    got = ctypes.c_int64(0)
+    check(L.crt_read_mbr_csv_device(str(path).encode(), n, r, ctypes.byref(box), ctypes.byref(got),
+                                    _stream_handle(stream)), "read_mbr_csv_device")
+    try:
+        out = BBox.empty(int(box.sz))
+        if box.sz:
+            for dst, src in ((out.xmin, box.xmin), (out.ymin, box.ymin), (out.xmax, box.xmax),
+                             (out.ymax, box.ymax), (out.id, box.id)):
+                _copy_ptr(dst.data_ptr(), src, 4 * int(box.sz))
+    finally:
+        L.crt_bbox_free(ctypes.byref(box))
+    return out
+
+
 def kernel_launches() -> int:
     return int(load().crt_kernel_launches())

@@ -256,6 +256,22 @@ int crt_plan_destroy(crt_plan plan);
  * parsed before the problem. */
 int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* ymin, float* xmax,
                      float* ymax, int32_t* id, int64_t* n_read);
+/* Replaces readMBR followed by box_h2d (src/utility.cpp:5-40,
+ * src/utility.cuh:42-66): the same format, values, statuses and *n_read as
+ * crt_read_mbr_csv, with the records found and parsed on the GPU.  The boxes
+ * land in newly cudaMalloc'd arrays *d_box (free with crt_bbox_free); n = -1
+ * reads every record of the file.  On an error nothing is allocated.
+ * Records the device parser cannot convert with certainty (hex or inf/nan
+ * spellings, values within a few double ulps of a float rounding boundary,
+ * malformed records, ...) are parsed by the host parser, so the result is
+ * always the host loader's.  Returns after the boxes are on the device. */
+int crt_read_mbr_csv_device(const char* path, int64_t n, float r, crt_bbox_f32* d_box,
+                            int64_t* n_read, crt_stream_t stream);
+/* The same for text already in host memory (len bytes), into the caller's
+ * device arrays of n entries. */
+int crt_parse_mbr_csv_device(const char* text, int64_t len, int64_t n, float r, float* d_xmin,
+                             float* d_ymin, float* d_xmax, float* d_ymax, int32_t* d_id,
+                             int64_t* n_read, crt_stream_t stream);
 
 /* Writes a built tree and its sorted box set to a file (no reference
  * counterpart; format in curtree_b200/csrc/io.cu). */

@@ -88,3 +88,21 @@ def test_read_mbr_errors():
         st, got, _, _ = read_ours(path, 3, 0.0)
         assert st == _lib.CRT_ERR_INVALID_ARG and got == 1
         assert b"record 1" in _lib.load().crt_last_error()
+
+
+def test_device_reader_argument_errors_need_no_gpu():
+    """crt_read_mbr_csv_device / crt_parse_mbr_csv_device reject bad
+    arguments, a missing file and a directory before touching a device."""
+    L = _lib.load()
+    box = _lib.crt_bbox_f32()
+    got = ctypes.c_int64(5)
+    with tempfile.TemporaryDirectory() as tmp:
+        for path, n in ((None, 1), (os.path.join(tmp, "missing.csv").encode(), 1), (tmp.encode(), 1),
+                        (os.path.join(tmp, "x.csv").encode(), -2)):
+            st = L.crt_read_mbr_csv_device(path, n, 0.0, ctypes.byref(box), ctypes.byref(got), None)
+            assert st == _lib.CRT_ERR_INVALID_ARG and got.value in (0, 5)
+            assert not box.xmin and box.sz == 0
+    assert L.crt_parse_mbr_csv_device(None, 10, 1, 0.0, None, None, None, None, None,
+                                      ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
+    assert L.crt_parse_mbr_csv_device(b"1,2,3,4,5,6,7\n", 14, 1, 0.0, None, None, None, None, None,
+                                      ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
