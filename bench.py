@@ -749,12 +749,28 @@ def ingest_leg(args, C, L, stream):
     boxes.id[:] = np.random.default_rng(22).integers(-2**31, 2**31 - 1, n)
     text = D.mbr_csv_text(boxes)
     nbytes = len(text)
+    sample = min(n, 500_000)
+    cut = int(np.flatnonzero(np.frombuffer(text, np.uint8) == 10)[sample - 1]) + 1
     shm = "/dev/shm" if os.path.isdir("/dev/shm") else None
     fd, path = tempfile.mkstemp(suffix=".csv", dir=shm)
+    fd2, path2 = tempfile.mkstemp(suffix=".csv", dir=shm)
+    ref = None
     try:
         with os.fdopen(fd, "wb") as f:
             f.write(text)
+        with os.fdopen(fd2, "wb") as f:
+            f.write(text[:cut])
         del text
+        # the reference's own readMBR (fscanf, one thread), built from its
+        # sources, on the first records: the CPU baseline of this leg
+        from oracle import oracle as O
+        if O.ref_cpu_available():
+            t0 = time.perf_counter()
+            O.ref_read_mbr(path2, sample, 0.0)
+            dt = time.perf_counter() - t0
+            ref = {"value": sample / dt, "unit": "records/s", "cores": 1, "kind": "reference",
+                   "sample": f"the first {sample} records, the reference's readMBR "
+                             "(src/utility.cpp:5-40) compiled from its sources, host arrays only"}
         box = _lib.crt_bbox_f32()
         got = ctypes.c_int64(0)
         h = ctypes.c_void_p(stream.cuda_stream)
@@ -817,6 +833,7 @@ def ingest_leg(args, C, L, stream):
         del src, dst
     finally:
         os.unlink(path)
+        os.unlink(path2)
     sec = statistics.median(secs)
     kern_ms = parts["ingest_lines"] + parts["ingest_emit"] + parts["ingest_parse"]
     return {"metric": "mbr_records_per_s", "value": n / sec, "unit": "records/s",
@@ -830,6 +847,7 @@ def ingest_leg(args, C, L, stream):
                             "cores": os.cpu_count(),
                             "what": "crt_read_mbr_csv (host threads) + copy of the five arrays"},
             "speedup_vs_host_loader": min(hsecs) / sec, "identical_to_host_loader": bool(identical),
+            "cpu_baseline": ref,
             "workload": f"{n // 10**6}M records 'x1,y1,x2,y2,id,pid,nume' (6 fraction digits, "
                         "corners half swapped, random int32 ids), file in the page cache, "
                         "crt_read_mbr_csv_device(path, n, r=0)"}
