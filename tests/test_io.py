@@ -106,3 +106,33 @@ def test_device_reader_argument_errors_need_no_gpu():
                                       ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
     assert L.crt_parse_mbr_csv_device(b"1,2,3,4,5,6,7\n", 14, 1, 0.0, None, None, None, None, None,
                                       ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
+
+
+def test_mbr_text_generator_matches_python_formatting():
+    """datasets.mbr_csv_text writes what Python's %.6f / %d would, and the
+    host loader reads it back to the same boxes."""
+    from curtree_b200 import datasets as D
+    rng = np.random.default_rng(8)
+    n = 3000
+    b = D.HostBoxes(*(rng.uniform(-4e4, 4e4, n).astype(np.float32) for _ in range(4)),
+                    rng.integers(-2**31, 2**31 - 1, n).astype(np.int32))
+    b.xmin[:3] = [0.0, -0.0000004, 123456.5]
+    b.id[:2] = [-2**31, 2**31 - 1]
+    text = D.mbr_csv_text(b, seed=9)
+    g = np.random.default_rng(9)
+    swap = g.random(n) < 0.5
+    pid, nume = g.integers(0, 100, n), g.integers(0, 10, n)
+    want = []
+    for i in range(n):
+        x1, y1, x2, y2 = ((b.xmax[i], b.ymax[i], b.xmin[i], b.ymin[i]) if swap[i]
+                          else (b.xmin[i], b.ymin[i], b.xmax[i], b.ymax[i]))
+        want.append(f"{x1:.6f},{y1:.6f},{x2:.6f},{y2:.6f},{b.id[i]},{pid[i]},{nume[i]}\n")
+    assert text.decode() == "".join(want)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "g.csv")
+        with open(path, "wb") as f:
+            f.write(text)
+        st, got, a, ids = read_ours(path, n, 0.0)
+        assert st == _lib.CRT_OK and got == n and np.array_equal(ids, b.id)
+        lo = np.minimum(b.xmin, b.xmax)
+        assert np.allclose(a[0], lo, rtol=0, atol=1e-2)
