@@ -424,7 +424,8 @@ __global__ void mbr_fix_kernel(const FixRecord* __restrict__ rec, int64_t c, flo
 // Host side
 // ---------------------------------------------------------------------------
 
-// Pinned staging slots, two per copy thread, kept for the life of the process.
+// Pinned staging slots, two per copy thread, allocated on first use and kept
+// for the life of the process.
 struct StagePool {
   std::mutex mu;
   char* slot[kStageThreads][2] = {};
@@ -493,21 +494,18 @@ int stage_text(char* d_text, Source& src, int dev)
 {
   const int64_t nchunks = cdiv(src.len, (int64_t)kStageChunk);
   if (nchunks == 0) return CRT_OK;
-  StagePool& P = stage_pool();
-  std::lock_guard<std::mutex> lock(P.mu);
-  if (!P.slot[0][0]) {
-    for (int t = 0; t < kStageThreads; t++)
-      for (int s = 0; s < 2; s++)
-        if (cudaHostAlloc((void**)&P.slot[t][s], kStageChunk, cudaHostAllocPortable) != cudaSuccess) {
-          cudaGetLastError();
-          for (int u = 0; u < kStageThreads; u++)
-            for (int v = 0; v < 2; v++)
-              if (P.slot[u][v]) cudaFreeHost(P.slot[u][v]), P.slot[u][v] = nullptr;
-          return fail(CRT_ERR_OOM, "read_mbr_csv_device: pinned staging allocation failed");
-        }
-  }
   const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
   const int nt = (int)std::min<int64_t>(std::min(kStageThreads, hw), nchunks);
+  StagePool& P = stage_pool();
+  std::lock_guard<std::mutex> lock(P.mu);
+  for (int t = 0; t < nt; t++)  // the slots of the threads this call uses
+    for (int s = 0; s < 2; s++)
+      if (!P.slot[t][s] &&
+          cudaHostAlloc((void**)&P.slot[t][s], kStageChunk, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        P.slot[t][s] = nullptr;
+        return fail(CRT_ERR_OOM, "read_mbr_csv_device: pinned staging allocation failed");
+      }
   std::vector<int> bad_read(nt, 0);
   std::vector<cudaError_t> err(nt, cudaSuccess);
   std::vector<std::thread> th;
