@@ -803,6 +803,25 @@ def ingest_leg(args, C, L, stream):
         dev_id = _d2h(box.id, n, np.int32)
         L.crt_bbox_free(ctypes.byref(box))
 
+        # the same boxes as 28-byte binary records
+        raw = D.mbr_bin_bytes(boxes)
+        with open(path2, "wb") as f:
+            f.write(raw)
+        bin_bytes = len(raw)
+        del raw
+        bsecs = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            _lib.check(L.crt_read_mbr_bin_device(path2.encode(), n, 0.0, ctypes.byref(box),
+                                                 ctypes.byref(got), h), "read_mbr_bin_device")
+            if i >= args.warmup:
+                bsecs.append(time.perf_counter() - t0)
+            L.crt_bbox_free(ctypes.byref(box))
+        binary = {"records_per_s": n / statistics.median(bsecs),
+                  "ms_per_step": statistics.median(bsecs) * 1e3, "file_bytes": bin_bytes,
+                  "gb_per_s": bin_bytes / statistics.median(bsecs) / 1e9,
+                  "what": "crt_read_mbr_bin_device, 28-byte records of the same boxes"}
+
         # the host loader, then the copy of its arrays to the device
         host = [np.empty(n, np.float32) for _ in range(4)]
         host_id = np.empty(n, np.int32)
@@ -847,7 +866,7 @@ def ingest_leg(args, C, L, stream):
                             "cores": os.cpu_count(),
                             "what": "crt_read_mbr_csv (host threads) + copy of the five arrays"},
             "speedup_vs_host_loader": min(hsecs) / sec, "identical_to_host_loader": bool(identical),
-            "cpu_baseline": ref,
+            "cpu_baseline": ref, "binary": binary,
             "workload": f"{n // 10**6}M records 'x1,y1,x2,y2,id,pid,nume' (6 fraction digits, "
                         "corners half swapped, random int32 ids), file in the page cache, "
                         "crt_read_mbr_csv_device(path, n, r=0)"}

@@ -117,6 +117,9 @@ SIGNATURES = {
     "crt_read_mbr_csv_device": (ctypes.c_int, [ctypes.c_char_p, _i64, ctypes.c_float,
                                                ctypes.POINTER(crt_bbox_f32), ctypes.POINTER(_i64),
                                                _vp]),
+    "crt_read_mbr_bin_device": (ctypes.c_int, [ctypes.c_char_p, _i64, ctypes.c_float,
+                                               ctypes.POINTER(crt_bbox_f32), ctypes.POINTER(_i64),
+                                               _vp]),
     "crt_parse_mbr_csv_device": (ctypes.c_int, [_vp, _i64, _i64, ctypes.c_float, _vp, _vp, _vp,
                                                 _vp, _vp, ctypes.POINTER(_i64), _vp]),
     "crt_tree_save": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(crt_rtree_f32),

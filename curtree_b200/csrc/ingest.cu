@@ -420,6 +420,29 @@ __global__ void mbr_fix_kernel(const FixRecord* __restrict__ rec, int64_t c, flo
   }
 }
 
+// Binary MBR records: 28 bytes each, little-endian float32 x1, y1, x2, y2 and
+// int32 id, pid, nume (the text record's fields in binary); the box is the one
+// readMBR makes of the text record.
+constexpr int64_t kBinRecord = 28;
+
+__global__ void __launch_bounds__(kParseThreads)
+    mbr_bin_kernel(const uint32_t* __restrict__ words, int64_t n, float r, float* __restrict__ xmin,
+                   float* __restrict__ ymin, float* __restrict__ xmax, float* __restrict__ ymax,
+                   int32_t* __restrict__ id)
+{
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t* w = words + 7 * k;
+    const float x1 = __uint_as_float(__ldg(w)), y1 = __uint_as_float(__ldg(w + 1));
+    const float x2 = __uint_as_float(__ldg(w + 2)), y2 = __uint_as_float(__ldg(w + 3));
+    xmin[k] = __fsub_rn(x2 < x1 ? x2 : x1, r);
+    ymin[k] = __fsub_rn(y2 < y1 ? y2 : y1, r);
+    xmax[k] = __fadd_rn(x1 < x2 ? x2 : x1, r);
+    ymax[k] = __fadd_rn(y1 < y2 ? y2 : y1, r);
+    id[k] = (int32_t)__ldg(w + 4);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -751,6 +774,60 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
   return CRT_OK;
 }
 
+// The binary loader: the first m records of the file staged to the device
+// like the text, then one thread per record.
+int ingest_bin(Source& src, int64_t n, float r, crt_bbox_f32* box_out, int64_t* n_read,
+               cudaStream_t stream)
+{
+  if (n_read) *n_read = 0;
+  if (src.len % kBinRecord)
+    return fail(CRT_ERR_INVALID_ARG, "read_mbr_bin_device: the file is not a whole number of "
+                                     "28-byte records");
+  const int64_t total = src.len / kBinRecord;
+  if (n > total) {
+    if (n_read) *n_read = total;
+    return fail(CRT_ERR_INVALID_ARG, "read_mbr_bin_device: file holds " + std::to_string(total) +
+                                         " records, " + std::to_string(n) + " requested");
+  }
+  const int64_t m = n < 0 ? total : n;
+  if (m > INT32_MAX) return fail(CRT_ERR_INVALID_ARG, "read_mbr_bin_device: more than 2^31-1 records");
+  crt_bbox_f32 box{};
+  box.sz = (int)m;
+  if (m > 0) {
+    int dev = 0;
+    CRT_CUDA(cudaGetDevice(&dev));
+    Scratch S(stream);
+    char* raw = S.get<char>((size_t)(m * kBinRecord) + 256);
+    if (!raw) return fail(CRT_ERR_OOM, "read_mbr_bin_device: device allocation failed");
+    char* d_rec = (char*)(((uintptr_t)raw + 255) & ~(uintptr_t)255);
+    CRT_CUDA(cudaStreamSynchronize(stream));  // the copy threads write d_rec on their own streams
+    src.len = m * kBinRecord;                 // only the records asked for
+    int rc = stage_text(d_rec, src, dev);
+    if (rc != CRT_OK) return rc;
+    void** dst[5] = {(void**)&box.xmin, (void**)&box.ymin, (void**)&box.xmax, (void**)&box.ymax,
+                     (void**)&box.id};
+    for (int a = 0; a < 5; a++)
+      if (cudaMalloc(dst[a], (size_t)m * 4) != cudaSuccess) {
+        cudaGetLastError();
+        for (int b = 0; b < a; b++) cudaFree(*dst[b]);
+        return fail(CRT_ERR_OOM, "read_mbr_bin_device: output allocation failed");
+      }
+    const int64_t grid = std::min<int64_t>(cdiv(m, kParseThreads), (int64_t)sm_count() * 16);
+    mbr_bin_kernel<<<(unsigned)grid, kParseThreads, 0, stream>>>(
+        (const uint32_t*)d_rec, m, r, box.xmin, box.ymin, box.xmax, box.ymax, box.id);
+    CRT_LAUNCHED(1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+      crt_bbox_free(&box);
+      return cuda_fail(e, "read_mbr_bin_device");
+    }
+  }
+  if (n_read) *n_read = m;
+  *box_out = box;
+  return CRT_OK;
+}
+
 }  // namespace
 
 }  // namespace crt
@@ -778,6 +855,31 @@ int crt_read_mbr_csv_device(const char* path, int64_t n, float r, crt_bbox_f32* 
     src.len = (int64_t)sb.st_size;
     crt_bbox_f32 box{};
     rc = ingest(src, n, r, true, Outputs{}, &box, n_read, (cudaStream_t)stream);
+    if (rc == CRT_OK) *d_box = box;
+  }
+  close(fd);
+  return rc;
+}
+
+int crt_read_mbr_bin_device(const char* path, int64_t n, float r, crt_bbox_f32* d_box,
+                            int64_t* n_read, crt_stream_t stream)
+{
+  if (!path || !d_box || n < -1) return fail(CRT_ERR_INVALID_ARG, "read_mbr_bin_device: bad arguments");
+  if (n_read) *n_read = 0;
+  const int fd = open(path, O_RDONLY | O_CLOEXEC);
+  if (fd < 0) return fail(CRT_ERR_INVALID_ARG, std::string("read_mbr_bin_device: cannot open ") + path);
+  struct stat sb;
+  if (fstat(fd, &sb) != 0 || !S_ISREG(sb.st_mode)) {
+    close(fd);
+    return fail(CRT_ERR_INVALID_ARG, std::string("read_mbr_bin_device: not a regular file: ") + path);
+  }
+  int rc;
+  {
+    Source src;
+    src.fd = fd;
+    src.len = (int64_t)sb.st_size;
+    crt_bbox_f32 box{};
+    rc = ingest_bin(src, n, r, &box, n_read, (cudaStream_t)stream);
     if (rc == CRT_OK) *d_box = box;
   }
   close(fd);

@@ -301,3 +301,26 @@ def mbr_csv_text(boxes: HostBoxes, decimals: int = 6, seed: int = 106) -> bytes:
         c += 1
     flat = np.ascontiguousarray(M.T).ravel()
     return flat[flat != 0].tobytes()
+
+
+MBR_BIN_RECORD = np.dtype([("x1", "<f4"), ("y1", "<f4"), ("x2", "<f4"), ("y2", "<f4"),
+                           ("id", "<i4"), ("pid", "<i4"), ("nume", "<i4")])
+
+
+def mbr_bin_bytes(boxes: HostBoxes, seed: int = 106) -> bytes:
+    """The boxes as 28-byte binary MBR records (float32 x1, y1, x2, y2, int32
+    id, pid, nume, little-endian): the fields of mbr_csv_text with the same
+    corner order and pid/nume draws, the corners kept exactly in fp32."""
+    rng = np.random.default_rng(seed)
+    n = boxes.n
+    swap = rng.random(n) < 0.5
+    rec = np.empty(n, MBR_BIN_RECORD)
+    f32 = lambda a: np.asarray(a, np.float32)
+    rec["x1"] = np.where(swap, f32(boxes.xmax), f32(boxes.xmin))
+    rec["y1"] = np.where(swap, f32(boxes.ymax), f32(boxes.ymin))
+    rec["x2"] = np.where(swap, f32(boxes.xmin), f32(boxes.xmax))
+    rec["y2"] = np.where(swap, f32(boxes.ymin), f32(boxes.ymax))
+    rec["id"] = boxes.id
+    rec["pid"] = rng.integers(0, 100, n)
+    rec["nume"] = rng.integers(0, 10, n)
+    return rec.tobytes()

@@ -394,11 +394,22 @@ def read_mbr_csv(path: str, n: int = -1, r: float = 0.0, stream=None) -> BBox:
     [min(y1,y2) - r, max(y1,y2) + r] with the fifth field as id.  n = -1 reads
     every record; otherwise exactly n records must be present.  A malformed
     record or a short file raises CrtError (the reference exits or throws)."""
+    return _read_mbr("crt_read_mbr_csv_device", path, n, r, stream)
+
+
+def read_mbr_bin(path: str, n: int = -1, r: float = 0.0, stream=None) -> BBox:
+    """The binary form of read_mbr_csv: 28-byte little-endian records of
+    float32 x1, y1, x2, y2 and int32 id, pid, nume (datasets.mbr_bin_bytes
+    writes them), the same boxes and ids as the text form of those values."""
+    return _read_mbr("crt_read_mbr_bin_device", path, n, r, stream)
+
+
+def _read_mbr(fn: str, path, n: int, r: float, stream) -> BBox:
     L = load()
     box = _lib.crt_bbox_f32()
     got = ctypes.c_int64(0)
-    check(L.crt_read_mbr_csv_device(str(path).encode(), n, r, ctypes.byref(box), ctypes.byref(got),
-                                    _stream_handle(stream)), "read_mbr_csv_device")
+    check(getattr(L, fn)(str(path).encode(), n, r, ctypes.byref(box), ctypes.byref(got),
+                         _stream_handle(stream)), fn)
     try:
         out = BBox.empty(int(box.sz))
         if box.sz:

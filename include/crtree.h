@@ -267,6 +267,15 @@ int crt_read_mbr_csv(const char* path, int64_t n, float r, float* xmin, float* y
  * always the host loader's.  Returns after the boxes are on the device. */
 int crt_read_mbr_csv_device(const char* path, int64_t n, float r, crt_bbox_f32* d_box,
                             int64_t* n_read, crt_stream_t stream);
+/* Binary form of the same records (no reference counterpart: the reference
+ * reads text only): a file of 28-byte little-endian records, float32 x1, y1,
+ * x2, y2 then int32 id, pid, nume, read into newly cudaMalloc'd arrays *d_box
+ * with readMBR's box [min(x1,x2) - r, max(x1,x2) + r] x [min(y1,y2) - r,
+ * max(y1,y2) + r] (free with crt_bbox_free).  n = -1 reads every record; a
+ * file size that is not a multiple of 28, or fewer than n records, is
+ * CRT_ERR_INVALID_ARG (*n_read = records present). */
+int crt_read_mbr_bin_device(const char* path, int64_t n, float r, crt_bbox_f32* d_box,
+                            int64_t* n_read, crt_stream_t stream);
 /* The same for text already in host memory (len bytes), into the caller's
  * device arrays of n entries. */
 int crt_parse_mbr_csv_device(const char* text, int64_t len, int64_t n, float r, float* d_xmin,

@@ -322,3 +322,88 @@ def test_python_reader_and_build(crt):
             crt.read_mbr_csv(path, n=len(rows) + 1)
         with pytest.raises(crt.CrtError):
             crt.read_mbr_csv(os.path.join(tmp, "missing.csv"))
+
+
+# ---- binary records ---------------------------------------------------------------
+
+def bin_read(path, n, r):
+    import torch
+    L = _lib.load()
+    box = _lib.crt_bbox_f32()
+    got = ctypes.c_int64(0)
+    st = L.crt_read_mbr_bin_device(str(path).encode(), n, r, ctypes.byref(box), ctypes.byref(got),
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    if st != _lib.CRT_OK:
+        assert not box.xmin and box.sz == 0
+        return st, got.value, None, None
+    from curtree_b200.rtree import _d2h
+    arrs = [_d2h(p, box.sz, np.float32) for p in (box.xmin, box.ymin, box.xmax, box.ymax)]
+    ids = _d2h(box.id, box.sz, np.int32)
+    assert L.crt_bbox_free(ctypes.byref(box)) == 0
+    return st, got.value, arrs, ids
+
+
+def expected_boxes(rec, r):
+    """readMBR's box of each binary record, in fp32 (std::min / std::max
+    keep the first endpoint unless the second compares below / above it)."""
+    r = np.float32(r)
+    x1, y1, x2, y2 = (rec[k] for k in ("x1", "y1", "x2", "y2"))
+    return [np.where(x2 < x1, x2, x1) - r, np.where(y2 < y1, y2, y1) - r,
+            np.where(x1 < x2, x2, x1) + r, np.where(y1 < y2, y2, y1) + r]
+
+
+def test_binary_records_match_readmbr_arithmetic(crt):
+    from curtree_b200 import datasets as D
+    rng = np.random.default_rng(12)
+    n = 700_001
+    rec = np.empty(n, D.MBR_BIN_RECORD)
+    for k in ("x1", "y1", "x2", "y2"):
+        rec[k] = rng.uniform(-1e5, 1e5, n).astype(np.float32)
+    special = np.array([np.nan, -np.nan, np.inf, -np.inf, 0.0, -0.0, 1e-45, -3.4e38], np.float32)
+    for k in ("x1", "y1", "x2", "y2"):
+        idx = rng.integers(0, n, 2000)
+        rec[k][idx] = special[rng.integers(0, len(special), 2000)]
+    rec["id"] = rng.integers(-2**31, 2**31 - 1, n)
+    rec["pid"], rec["nume"] = 1, 2
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "m.bin")
+        rec.tofile(path)
+        for r in (0.0, 0.37):
+            st, got, a, ids = bin_read(path, -1, r)
+            assert (st, got) == (_lib.CRT_OK, n)
+            for mine, want in zip(a, expected_boxes(rec, r)):
+                assert np.array_equal(mine.view(np.uint32), want.view(np.uint32))
+            assert np.array_equal(ids, rec["id"])
+        st, got, a, ids = bin_read(path, 1000, 1.0)
+        assert (st, got, len(ids)) == (_lib.CRT_OK, 1000, 1000)
+        assert np.array_equal(ids, rec["id"][:1000])
+        assert bin_read(path, n + 1, 0.0)[:2] == (_lib.CRT_ERR_INVALID_ARG, n)
+        with open(path, "ab") as f:
+            f.write(b"\0" * 5)
+        assert bin_read(path, -1, 0.0)[0] == _lib.CRT_ERR_INVALID_ARG
+        open(path, "wb").close()
+        st, got, a, ids = bin_read(path, -1, 0.0)
+        assert (st, got, len(ids)) == (_lib.CRT_OK, 0, 0)
+
+
+def test_binary_and_text_forms_agree(crt):
+    """The same boxes written as text (nine significant digits: exact in
+    fp32) and as binary records load to identical device boxes."""
+    from curtree_b200 import datasets as D
+    b = D.uniform_boxes(200_000, seed=31)
+    b.id[:] = np.random.default_rng(32).integers(-2**31, 2**31 - 1, b.n)
+    raw = D.mbr_bin_bytes(b, seed=5)
+    rec = np.frombuffer(raw, D.MBR_BIN_RECORD)
+    with tempfile.TemporaryDirectory() as tmp:
+        pb, pt = os.path.join(tmp, "m.bin"), os.path.join(tmp, "m.csv")
+        with open(pb, "wb") as f:
+            f.write(raw)
+        with open(pt, "w") as f:
+            f.write("".join(f"{x1:.9g},{y1:.9g},{x2:.9g},{y2:.9g},{i},{p},{q}\n"
+                            for x1, y1, x2, y2, i, p, q in rec.tolist()))
+        same(device_read(pt, b.n, 0.5), bin_read(pb, b.n, 0.5))
+        x = crt.read_mbr_bin(pb, r=0.5).to_host()
+        y = crt.read_mbr_csv(pt, r=0.5).to_host()
+        for u, v in zip((x.xmin, x.ymin, x.xmax, x.ymax), (y.xmin, y.ymin, y.xmax, y.ymax)):
+            assert np.array_equal(u.view(np.uint32), v.view(np.uint32))
+        assert np.array_equal(x.id, b.id) and np.array_equal(y.id, b.id)

@@ -136,3 +136,25 @@ def test_mbr_text_generator_matches_python_formatting():
         assert st == _lib.CRT_OK and got == n and np.array_equal(ids, b.id)
         lo = np.minimum(b.xmin, b.xmax)
         assert np.allclose(a[0], lo, rtol=0, atol=1e-2)
+
+
+def test_binary_reader_size_errors_need_no_gpu():
+    """crt_read_mbr_bin_device checks the file's size against whole 28-byte
+    records and against n before touching a device."""
+    L = _lib.load()
+    box = _lib.crt_bbox_f32()
+    got = ctypes.c_int64(0)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "m.bin")
+        with open(path, "wb") as f:
+            f.write(b"\0" * (28 * 3 + 1))
+        assert L.crt_read_mbr_bin_device(path.encode(), -1, 0.0, ctypes.byref(box),
+                                         ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
+        with open(path, "wb") as f:
+            f.write(b"\0" * (28 * 3))
+        assert L.crt_read_mbr_bin_device(path.encode(), 4, 0.0, ctypes.byref(box),
+                                         ctypes.byref(got), None) == _lib.CRT_ERR_INVALID_ARG
+        assert got.value == 3 and not box.xmin
+        assert L.crt_read_mbr_bin_device(os.path.join(tmp, "none").encode(), 1, 0.0,
+                                         ctypes.byref(box), ctypes.byref(got),
+                                         None) == _lib.CRT_ERR_INVALID_ARG
