@@ -370,6 +370,22 @@ __device__ __forceinline__ bool record_fast(const uint8_t* t, int64_t p, float v
   return true;
 }
 
+// a - r and a + r with the host's NaN rule: x86 arithmetic returns the NaN
+// operand itself, quieted (the first one when both are NaN), where the GPU
+// returns its canonical NaN; readMBR runs on the host, so its boxes keep the
+// input NaN's sign and payload.
+__device__ __forceinline__ float quiet_nan(float x) { return __int_as_float(__float_as_int(x) | 0x400000); }
+
+__device__ __forceinline__ float sub_host(float a, float r)
+{
+  return isnan(a) ? quiet_nan(a) : isnan(r) ? quiet_nan(r) : __fsub_rn(a, r);
+}
+
+__device__ __forceinline__ float add_host(float a, float r)
+{
+  return isnan(a) ? quiet_nan(a) : isnan(r) ? quiet_nan(r) : __fadd_rn(a, r);
+}
+
 __global__ void __launch_bounds__(kParseThreads, 4)
     mbr_parse_kernel(const uint8_t* __restrict__ text, const int64_t* __restrict__ starts, int64_t m,
                      float r, float* __restrict__ xmin, float* __restrict__ ymin,
@@ -384,10 +400,10 @@ __global__ void __launch_bounds__(kParseThreads, 4)
     int32_t rid = 0;
     if (record_fast(text, s, v, rid)) {
       // readMBR: std::min / std::max of the endpoints, then -/+ r in fp32
-      xmin[k] = __fsub_rn(v[2] < v[0] ? v[2] : v[0], r);
-      ymin[k] = __fsub_rn(v[3] < v[1] ? v[3] : v[1], r);
-      xmax[k] = __fadd_rn(v[0] < v[2] ? v[2] : v[0], r);
-      ymax[k] = __fadd_rn(v[1] < v[3] ? v[3] : v[1], r);
+      xmin[k] = sub_host(v[2] < v[0] ? v[2] : v[0], r);
+      ymin[k] = sub_host(v[3] < v[1] ? v[3] : v[1], r);
+      xmax[k] = add_host(v[0] < v[2] ? v[2] : v[0], r);
+      ymax[k] = add_host(v[1] < v[3] ? v[3] : v[1], r);
       id[k] = rid;
     } else {
       const unsigned long long j = atomicAdd(n_fallback, 1ull);
@@ -435,10 +451,10 @@ __global__ void __launch_bounds__(kParseThreads)
     const uint32_t* w = words + 7 * k;
     const float x1 = __uint_as_float(__ldg(w)), y1 = __uint_as_float(__ldg(w + 1));
     const float x2 = __uint_as_float(__ldg(w + 2)), y2 = __uint_as_float(__ldg(w + 3));
-    xmin[k] = __fsub_rn(x2 < x1 ? x2 : x1, r);
-    ymin[k] = __fsub_rn(y2 < y1 ? y2 : y1, r);
-    xmax[k] = __fadd_rn(x1 < x2 ? x2 : x1, r);
-    ymax[k] = __fadd_rn(y1 < y2 ? y2 : y1, r);
+    xmin[k] = sub_host(x2 < x1 ? x2 : x1, r);
+    ymin[k] = sub_host(y2 < y1 ? y2 : y1, r);
+    xmax[k] = add_host(x1 < x2 ? x2 : x1, r);
+    ymax[k] = add_host(y1 < y2 ? y2 : y1, r);
     id[k] = (int32_t)__ldg(w + 4);
   }
 }
