@@ -345,7 +345,9 @@ def bin_read(path, n, r):
 
 def expected_boxes(rec, r):
     """readMBR's box of each binary record, in fp32 (std::min / std::max
-    keep the first endpoint unless the second compares below / above it)."""
+    keep the first endpoint unless the second compares below / above it).
+    numpy computes on the host, like readMBR, so a NaN corner keeps its sign
+    and payload here; the device must do the same."""
     r = np.float32(r)
     x1, y1, x2, y2 = (rec[k] for k in ("x1", "y1", "x2", "y2"))
     return [np.where(x2 < x1, x2, x1) - r, np.where(y2 < y1, y2, y1) - r,
