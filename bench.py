@@ -181,6 +181,34 @@ def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7):
             "sample": f"{n} of {windows.n} windows x {boxes.n} boxes, {t:.1f} s, {pairs} pairs"}
 
 
+def cpu_rtree_rate(h_tree, h_sorted, windows, seconds: float, rng_seed: int = 9):
+    """Windows/s of a CPU R-tree on all host threads: the same packed tree
+    (the reference's layout, copied from the device) searched depth-first by
+    the oracle's C restatement of the reference's tree query, counting hits
+    and pair digests without writing pairs.  It stands in for the reference's
+    Boost R-tree check (src/verify.hpp:35-104), whose Boost dependency is
+    absent; a sample of windows sized to about `seconds` of CPU work."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(rng_seed)
+
+    def run(m):
+        idx = np.sort(rng.choice(windows.n, size=min(m, windows.n), replace=False))
+        q = windows.take(idx)
+        t0 = time.perf_counter()
+        st = O.tree_query_stats(h_tree, h_sorted, q, nthreads=threads)
+        return q.n, time.perf_counter() - t0, st.total
+
+    n0, t0, _ = run(threads * 8)
+    m = int(max(threads, min(windows.n, n0 / max(t0, 1e-6) * seconds)))
+    m = (m + threads - 1) // threads * threads
+    n, t, pairs = run(m)
+    return {"value": n / t, "unit": "windows/s", "cores": threads, "kind": "port",
+            "sample": f"{n} of {windows.n} windows x {h_sorted.n} boxes, {t:.1f} s, {pairs} pairs",
+            "what": "depth-first search of the same packed tree on the host (oracle restatement "
+                    "of the reference's query), hits counted, no pair writes"}
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -355,6 +383,11 @@ def run_ours(args, rank, world, dist):
                         "windows_per_s": world * args.windows / (pms / args.steps / 1e3),
                         "kernel_ms": pk_ms / max(args.steps, 1)}
         del offs
+
+    # ---- CPU R-tree on the same tree (rank 0 of a 1-GPU run) ------------------
+    if "cpu" not in skip and rank == 0 and world == 1:
+        out["cpu_rtree"] = cpu_rtree_rate(rt.to_host(), sorted_box.to_host(), windows,
+                                          args.cpu_seconds)
 
     # ---- end to end through the C ABI with host buffers ----------------------
     if "e2e" not in skip:
@@ -976,7 +1009,7 @@ def main():
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
                 "plain": out.get("plain"), "build": out.get("build"),
                 "serving": out.get("serving"), "adversarial": out.get("adversarial"),
-                "ingest": out.get("ingest"),
+                "ingest": out.get("ingest"), "cpu_rtree": out.get("cpu_rtree"),
                 "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                 "persistent_kernel_ms": p["kernel_ms"]}
         if "plain" in out:
