@@ -386,8 +386,11 @@ def run_ours(args, rank, world, dist):
 
     # ---- CPU R-tree on the same tree (rank 0 of a 1-GPU run) ------------------
     if "cpu" not in skip and rank == 0 and world == 1:
-        out["cpu_rtree"] = cpu_rtree_rate(rt.to_host(), sorted_box.to_host(), windows,
-                                          args.cpu_seconds)
+        try:
+            out["cpu_rtree"] = cpu_rtree_rate(rt.to_host(), sorted_box.to_host(), windows,
+                                              args.cpu_seconds)
+        except Exception as e:  # a side figure: report it, keep the line
+            out["cpu_rtree"] = {"error": f"{type(e).__name__}: {e}"}
 
     # ---- end to end through the C ABI with host buffers ----------------------
     if "e2e" not in skip:
