@@ -92,6 +92,78 @@ bool parse_mbr_record(const char* p, const char* end, float v[4], int& id)
   return true;
 }
 
+namespace {
+
+// Class of a stretch's last byte that is not ' ', '\t' or '\r'.
+constexpr int kNoByte = 0, kNewline = 1, kOtherByte = 2;
+
+inline bool is_blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
+
+int last_class(const char* p, const char* e)
+{
+  while (e > p) {
+    const char c = *--e;
+    if (!is_blank(c)) return c == '\n' ? kNewline : kOtherByte;
+  }
+  return kNoByte;
+}
+
+// Record starts in [b, e), at most `cap`, given the class of the last
+// non-blank byte before b.
+void chunk_starts(const char* base, size_t b, size_t e, int in, int64_t cap,
+                  std::vector<size_t>& out)
+{
+  int prev = in;
+  for (size_t i = b; i < e && (int64_t)out.size() < cap; i++) {
+    const char c = base[i];
+    if (is_blank(c)) continue;
+    if (c != '\n' && prev != kOtherByte) out.push_back(i);
+    prev = c == '\n' ? kNewline : kOtherByte;
+  }
+}
+
+}  // namespace
+
+// The first n record starts: the first byte of each line that is not ' ',
+// '\t' or '\r', unless it is the line's '\n' -- the same as "a byte that is
+// neither blank nor '\n' whose previous non-blank byte is a '\n' or absent".
+// The second form splits: host threads take 8 MiB chunks, the class each
+// chunk ends with is carried across the chunks, then each thread lists its
+// chunk's starts.
+std::vector<size_t> record_starts(const char* base, size_t L, int64_t n)
+{
+  constexpr size_t kChunk = size_t(8) << 20;
+  const int hw = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)hw, (L + kChunk - 1) / kChunk));
+  const size_t per = (L + nt - 1) / std::max(nt, 1);
+  std::vector<int> last(nt, kNoByte);
+  std::vector<std::vector<size_t>> part(nt);
+  auto run = [&](auto&& body) {
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(body, t);
+    body(0);
+    for (auto& x : th) x.join();
+  };
+  run([&](int t) {
+    const size_t b = std::min(L, t * per), e = std::min(L, b + per);
+    last[t] = last_class(base + b, base + e);
+  });
+  run([&](int t) {
+    int in = kNoByte;
+    for (int u = 0; u < t; u++)
+      if (last[u] != kNoByte) in = last[u];
+    const size_t b = std::min(L, t * per), e = std::min(L, b + per);
+    chunk_starts(base, b, e, in, n, part[t]);
+  });
+  std::vector<size_t> starts;
+  starts.reserve((size_t)std::max<int64_t>(0, n));
+  for (int t = 0; t < nt && (int64_t)starts.size() < n; t++) {
+    const size_t take = (size_t)std::min<int64_t>((int64_t)part[t].size(), n - (int64_t)starts.size());
+    starts.insert(starts.end(), part[t].begin(), part[t].begin() + take);
+  }
+  return starts;
+}
+
 void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, float* ymax)
 {
   // readMBR: min/max of the endpoints, then -/+ r (fp32)
@@ -104,17 +176,7 @@ void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, f
 int read_mbr_text(const char* base, size_t L, int64_t n, float r, float* xmin, float* ymin,
                   float* xmax, float* ymax, int32_t* id, int64_t* n_read)
 {
-  // record starts: non-empty lines
-  std::vector<size_t> starts;
-  starts.reserve((size_t)n);
-  size_t i = 0;
-  while (i < L && (int64_t)starts.size() < n) {
-    size_t j = i;
-    while (j < L && (base[j] == ' ' || base[j] == '\t' || base[j] == '\r')) j++;
-    if (j < L && base[j] != '\n') starts.push_back(j);
-    while (i < L && base[i] != '\n') i++;
-    i++;
-  }
+  const std::vector<size_t> starts = record_starts(base, L, n);
   const int64_t m = (int64_t)starts.size();
   const char* end = base + L;
   int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));

@@ -158,3 +158,33 @@ def test_binary_reader_size_errors_need_no_gpu():
         assert L.crt_read_mbr_bin_device(os.path.join(tmp, "none").encode(), 1, 0.0,
                                          ctypes.byref(box), ctypes.byref(got),
                                          None) == _lib.CRT_ERR_INVALID_ARG
+
+
+@pytest.mark.skipif(not O.ref_cpu_available(), reason="reference CPU build absent")
+def test_multi_chunk_file_matches_reference():
+    """A file large enough for the record-start scan to split across host
+    threads (8 MiB chunks), with blank lines, CRLF ends, indented records and
+    a blank stretch longer than a chunk, reads like the reference's readMBR."""
+    rng = np.random.default_rng(17)
+    rows = make_rows(400_000, seed=18)
+    seps = ["\n", "\r\n", "\n\n", "\n   \n", "\n\t \r\n", "\n  "]
+    parts = []
+    for i, r in enumerate(rows):
+        parts.append(FORMATS["plain"](r))
+        parts.append(seps[rng.integers(0, len(seps))])
+        if i == 150_000:
+            parts.append(" \t\r\n" * (3 << 20))  # 12 MiB without a record
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "big.csv")
+        with open(path, "w") as f:
+            f.write("".join(parts))
+        assert os.path.getsize(path) > 3 * (8 << 20)
+        for n in (len(rows), 150_002, 1):
+            ref = O.ref_read_mbr(path, n, 0.5)
+            st, got, a, ids = read_ours(path, n, 0.5)
+            assert st == _lib.CRT_OK and got == n
+            for mine, theirs in zip(a, (ref.xmin, ref.ymin, ref.xmax, ref.ymax)):
+                assert np.array_equal(mine.view(np.uint32), theirs.view(np.uint32))
+            assert np.array_equal(ids, ref.id)
+        st, got, _, _ = read_ours(path, len(rows) + 1, 0.5)
+        assert (st, got) == (_lib.CRT_ERR_INVALID_ARG, len(rows))
