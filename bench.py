@@ -70,7 +70,8 @@ def parse():
     p.add_argument("--autotune", type=int, default=1, help="pick fanout/warps/staging first (untimed)")
     p.add_argument("--autotune-windows", type=int, default=100_000)
     p.add_argument("--skip", default="",
-                   help="comma list of legs to skip: build,e2e,plain,cpu,serve,adversarial")
+                   help="comma list of legs to skip: build,e2e,plain,cpu,serve,adversarial,"
+                        "ingest,config1")
     p.add_argument("--adv-boxes", type=int, default=50_000_000)
     p.add_argument("--adv-windows", type=int, default=2_000_000)
     p.add_argument("--adv-buffer-log2", type=int, default=32,
@@ -78,11 +79,24 @@ def parse():
     p.add_argument("--ingest-records", type=int, default=4_000_000,
                    help="records of the MBR text file the ingest leg reads")
     p.add_argument("--serve-trees", default="1000000,5000000,20000000,50000000")
-    p.add_argument("--serve-requests", type=int, default=400)
-    p.add_argument("--serve-rates", default="1000,3000,10000",
+    p.add_argument("--serve-requests", type=int, default=2000)
+    p.add_argument("--serve-rates", default="1000,3000,10000,30000,100000",
                    help="comma list of Poisson arrival rates (requests/s)")
     p.add_argument("--serve-max-batch", type=int, default=100_000)
     p.add_argument("--serve-arena-gb", type=int, default=64)
+    p.add_argument("--parity", type=int, default=1,
+                   help="check the GPU's pairs against the oracle (untimed; per-window digests)")
+    p.add_argument("--parity-windows", type=int, default=0,
+                   help="windows of the headline batch the oracle checks (0: all at one GPU, "
+                        "100k per rank under torchrun)")
+    p.add_argument("--parity-adv-windows", type=int, default=50_000,
+                   help="windows of the adversarial batch the oracle checks")
+    p.add_argument("--parity-serve-every", type=int, default=8,
+                   help="the oracle checks every k-th served request")
+    p.add_argument("--reference-gpu", type=int, default=1,
+                   help="reference arm: also time the reference's own GPU path (oracle/_ref)")
+    p.add_argument("--detail", default="",
+                   help="also write the full result (autotune table, every leg) to this JSON file")
     return p.parse_args()
 
 
@@ -149,10 +163,12 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # reference CPU path (bounded sample)
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7):
+def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7, keep=False):
     """Windows/s of the reference's nested_loop_query over all host threads,
     on a sample of windows sized to about `seconds` of CPU work.  Falls back to
-    the oracle's restatement when the reference build is absent."""
+    the oracle's restatement when the reference build is absent.  keep: also
+    return the sample's window indices with the per-window pair counts and
+    digests of the pairs the reference emitted (for the parity check)."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     kind = "reference" if O.ref_cpu_available() else "port"
@@ -161,24 +177,23 @@ def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7):
     def run(m):
         idx = np.sort(rng.choice(windows.n, size=min(m, windows.n), replace=False))
         q = windows.take(idx)
-        qid = np.arange(q.n, dtype=np.int32)
-        t0 = time.perf_counter()
         if kind == "reference":
-            R = O.ref_cpu()
-            a = [np.ascontiguousarray(x) for x in (q.xmin, q.ymin, q.xmax, q.ymax)]
-            d = [np.ascontiguousarray(x) for x in (boxes.xmin, boxes.ymin, boxes.xmax, boxes.ymax)]
-            pairs = R.ref_nested_loop_query_mt(*a, qid, q.n, *d, boxes.id, boxes.n, threads)
+            c, h, pairs, t = O.ref_nested_loop_digest(q, boxes, idx.astype(np.int32), threads)
         else:
-            c, _ = O.nested_loop_stats(q, boxes, nthreads=threads)
+            t0 = time.perf_counter()
+            c, h = O.nested_loop_stats(q, boxes, nthreads=threads)
+            t = time.perf_counter() - t0
+            h = None  # positional digests: not comparable with window indices
             pairs = int(c.sum())
-        return q.n, time.perf_counter() - t0, int(pairs)
+        return q.n, t, int(pairs), (idx, c, h)
 
-    n0, t0, _ = run(threads)
+    n0, t0, _, _ = run(threads)
     m = int(max(threads, min(windows.n, n0 / max(t0, 1e-6) * seconds)))
     m = (m + threads - 1) // threads * threads
-    n, t, pairs = run(m)
-    return {"value": n / t, "unit": "windows/s", "cores": threads, "kind": kind,
-            "sample": f"{n} of {windows.n} windows x {boxes.n} boxes, {t:.1f} s, {pairs} pairs"}
+    n, t, pairs, kept = run(m)
+    out = {"value": n / t, "unit": "windows/s", "cores": threads, "kind": kind,
+           "sample": f"{n} of {windows.n} windows x {boxes.n} boxes, {t:.1f} s, {pairs} pairs"}
+    return (out, kept) if keep else out
 
 
 def cpu_rtree_rate(h_tree, h_sorted, windows, seconds: float, rng_seed: int = 9):
@@ -207,6 +222,45 @@ def cpu_rtree_rate(h_tree, h_sorted, windows, seconds: float, rng_seed: int = 9)
             "sample": f"{n} of {windows.n} windows x {h_sorted.n} boxes, {t:.1f} s, {pairs} pairs",
             "what": "depth-first search of the same packed tree on the host (oracle restatement "
                     "of the reference's query), hits counted, no pair writes"}
+
+
+# ---------------------------------------------------------------------------
+# parity at full size (untimed): per-window pair counts and order-independent
+# digests of what the GPU wrote, against the oracle's tree query on the
+# oracle's own build of the same boxes, and against the reference's own
+# brute force (nested_loop_query) on the CPU baseline's sample.  This is the
+# reference drivers' check (sort both pair vectors, compare them:
+# src/rtree_test_frontier.cu:102-123) in a form that holds at 10^9-10^11 pairs.
+# ---------------------------------------------------------------------------
+def same_tree(h_tree, h_sorted, tr, sb) -> bool:
+    keys = ("xmin", "ymin", "xmax", "ymax", "pos", "len")
+    ok = all(np.array_equal(np.asarray(getattr(h_tree, k)).view(np.int32),
+                            np.asarray(getattr(tr, k)).view(np.int32)) for k in keys)
+    return bool(ok and all(np.array_equal(np.asarray(getattr(h_sorted, k)).view(np.int32),
+                                          np.asarray(getattr(sb, k)).view(np.int32))
+                           for k in ("xmin", "ymin", "xmax", "ymax", "id")))
+
+
+def compare_digests(got_c, got_h, want_c, want_h) -> dict:
+    bad = (got_c != want_c) | (got_h != want_h)
+    return {"windows": int(want_c.size), "pairs": int(want_c.sum()),
+            "counts_ok": bool(np.array_equal(got_c, want_c)),
+            "digest_ok": bool(not bad.any()), "windows_differing": int(bad.sum())}
+
+
+def sample_indices(n: int, m: int) -> np.ndarray:
+    """All of [0, n) when m <= 0 or m >= n, else m indices spread evenly."""
+    if m <= 0 or m >= n:
+        return np.arange(n, dtype=np.int32)
+    return np.unique(np.linspace(0, n - 1, m).astype(np.int64)).astype(np.int32)
+
+
+def oracle_tree(boxes, fanout, rt, sorted_box):
+    """The oracle's build of the same boxes and whether the GPU's tree and
+    permuted boxes equal it bit for bit."""
+    from oracle import oracle as O
+    sb, tr = O.build(boxes, fanout)
+    return sb, tr, same_tree(rt.to_host(), sorted_box.to_host(), tr, sb)
 
 
 # ---------------------------------------------------------------------------
@@ -259,6 +313,24 @@ def timed(fn, steps, stream):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1)
+
+
+def per_step_ms(fn, steps, stream):
+    """Device time of each of `steps` consecutive steps (events between them)."""
+    import torch
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for i in range(steps):
+        fn()
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    return [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+
+
+def latency_summary(ms):
+    return {"batches": len(ms), "p50_ms": float(np.percentile(ms, 50)),
+            "p99_ms": float(np.percentile(ms, 99)), "max_ms": float(max(ms))}
 
 
 def profile_collect(name):
@@ -363,6 +435,18 @@ def run_ours(args, rank, world, dist):
     out["workload_stats"] = {"pairs": pairs, "leaf_boxes_tested_reference": tested,
                              "leaf_boxes_tested": tested_c, "pairs_from_contained_ranges": st["range_hits"],
                              "pairs_per_window": pairs / args.windows}
+    # single-batch latency of the persistent form (untimed: each step alone)
+    out["persistent"]["batch_latency"] = latency_summary(
+        per_step_ms(plan.launch, max(args.steps, 20), stream))
+    digests = {}
+    if args.parity:
+        # per-window counts and digests of the pairs the last launch wrote
+        r = C.read_result(res)
+        assert r["overflow"] == 0 and r["count"] == pairs, r
+        dg = C.PairDigest(args.windows)
+        dg.add(fid, tid, n=pairs)
+        digests["persistent"] = dg.to_host()
+        del dg
     plan.destroy()
 
     # ---- plain form ---------------------------------------------------------
@@ -381,8 +465,28 @@ def run_ours(args, rank, world, dist):
         pms = reduce_max(pms, dist)
         out["plain"] = {"ms_per_step": pms / args.steps,
                         "windows_per_s": world * args.windows / (pms / args.steps / 1e3),
-                        "kernel_ms": pk_ms / max(args.steps, 1)}
+                        "kernel_ms": pk_ms / max(args.steps, 1),
+                        "batch_latency": latency_summary(per_step_ms(plain, max(args.steps, 20),
+                                                                     stream))}
+        if args.parity:
+            r = C.read_result(res)
+            assert r["overflow"] == 0 and r["count"] == pairs, r
+            dg = C.PairDigest(args.windows)
+            dg.add(fid, tid, n=pairs)
+            digests["plain"] = dg.to_host()
+            del dg
         del offs
+
+    # ---- parity of the headline batch against the oracle (untimed) -----------
+    if args.parity:
+        out["parity"] = parity_headline(args, boxes, windows, rt, sorted_box, digests, world)
+        out["_digests"] = digests
+        if dist is not None:  # every rank checked its own batch: all must agree
+            import torch
+            ok = torch.tensor([1 if out["parity"]["ok"] else 0], dtype=torch.int32, device="cuda")
+            dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+            out["parity"]["ok"] = bool(ok.item())
+            out["parity"]["ranks"] = world
 
     # ---- CPU R-tree on the same tree (rank 0 of a 1-GPU run) ------------------
     if "cpu" not in skip and rank == 0 and world == 1:
@@ -416,10 +520,41 @@ def run_ours(args, rank, world, dist):
         out["ingest"] = ingest_leg(args, C, L, stream)
         torch.cuda.empty_cache()
 
+    # ---- the reference's own small case through the drop-in calls -----------------
+    if "config1" not in skip and rank == 0:
+        out["config1"] = config1_leg(args, C, stream)
+        torch.cuda.empty_cache()
+
     # ---- bulk load ------------------------------------------------------------
     if "build" not in skip:
         out["build"] = build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world)
     return out, boxes, windows
+
+
+def parity_headline(args, boxes, windows, rt, sorted_box, digests, world):
+    """The oracle's build of the headline boxes against the GPU's tree (bit
+    for bit), and the oracle's tree query on its own tree against the
+    per-window counts and digests of each GPU form's output: every window at
+    one GPU, a spread sample per rank under torchrun."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    sb, tr, tree_ok = oracle_tree(boxes, args.fanout, rt, sorted_box)
+    m = args.parity_windows if args.parity_windows > 0 else (0 if world == 1 else 100_000)
+    idx = sample_indices(windows.n, m)
+    q = windows if idx.size == windows.n else windows.take(idx)
+    want = O.tree_query_stats(tr, sb, q, qid=idx)
+    forms = {}
+    for name, (c, h, bad) in digests.items():
+        forms[name] = dict(compare_digests(c[idx], h[idx], want.counts, want.hashes),
+                           pairs_outside_windows=bad,
+                           total_pairs_ok=bool(int(c.sum()) == int(want.counts.sum()))
+                           if idx.size == windows.n else None)
+    ok = tree_ok and all(f["digest_ok"] and f["pairs_outside_windows"] == 0 for f in forms.values())
+    return {"ok": bool(ok), "tree_identical": tree_ok, "windows_checked": int(idx.size),
+            "pairs_checked": int(want.counts.sum()), "forms": forms,
+            "oracle": "oracle/crt_oracle.c build + tree query (src/rtree_bulkload_thrust.cuh, "
+                      "src/rtree_bfs_frontier.cuh semantics) on the host",
+            "seconds": time.perf_counter() - t0}
 
 
 def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, dist, world):
@@ -559,9 +694,10 @@ def serving_workload(args, rank):
     return trees, reqs, gaps
 
 
-def serve_run(srv, tids, reqs, arrivals):
+def serve_run(srv, tids, reqs, arrivals, on_done=None):
     """Replays one arrival schedule through the server; returns latencies
-    (arrival to completion), makespan, pairs and retries."""
+    (arrival to completion), makespan, pairs and retries.  on_done(i, c) sees
+    each completion before its release."""
     import time
     lat = np.zeros(len(reqs))
     pairs = retries = 0
@@ -589,6 +725,8 @@ def serve_run(srv, tids, reqs, arrivals):
             lat[i] = c["complete_time_s"] - (t0 + arrivals[i])
             pairs += c["count"]
             retries += c["retries"]
+            if on_done is not None:
+                on_done(i, c)
             srv.release(c["request_id"])
             done += 1
         if nxt < len(reqs) and not backlog:
@@ -613,6 +751,47 @@ def plain_run(C, built, reqs, arrivals, stats, fid, tid, res, h_res):
         assert r["count"] == stats[i], (r, stats[i])
         lat[i] = time.monotonic() - (t0 + arrivals[i])
     return lat, time.monotonic() - t0
+
+
+def serving_parity(args, C, srv, tids, trees, built, reqs):
+    """Every k-th request served again (untimed, as fast as admitted), each
+    completion's pairs digested on the device by window, against the
+    oracle's tree query on the oracle's own build of that tree."""
+    import torch
+
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    chk = list(range(0, len(reqs), max(1, args.parity_serve_every)))
+    got = {}
+
+    def digest(k, c):
+        dg = C.PairDigest(reqs[chk[k]][1].n)
+        dg.add_ptr(c["d_fid"], c["d_tid"], c["count"])
+        torch.cuda.current_stream().synchronize()  # read before the release
+        got[chk[k]] = dg.to_host()
+
+    serve_run(srv, tids, [reqs[i] for i in chk], np.zeros(len(chk)), on_done=digest)
+    oracle = {}
+    trees_ok = True
+    for ti in sorted({reqs[i][0] for i in chk}):
+        sb, tr, ok = oracle_tree(trees[ti], args.fanout, built[ti][0], built[ti][1])
+        oracle[ti] = (sb, tr)
+        trees_ok = trees_ok and ok
+    bad_req = windows = pairs = outside = 0
+    for i in chk:
+        ti, w = reqs[i]
+        want = O.tree_query_stats(oracle[ti][1], oracle[ti][0], w)
+        c, h, nb = got[i]
+        outside += nb
+        windows += w.n
+        pairs += int(want.counts.sum())
+        if not (np.array_equal(c, want.counts) and np.array_equal(h, want.hashes)):
+            bad_req += 1
+    return {"ok": bool(trees_ok and bad_req == 0 and outside == 0), "trees_identical": trees_ok,
+            "requests_checked": len(chk), "requests_differing": bad_req, "windows_checked": windows,
+            "pairs_checked": pairs, "pairs_outside_windows": outside,
+            "sample": f"every {max(1, args.parity_serve_every)}th request, replayed untimed",
+            "seconds": time.perf_counter() - t0}
 
 
 def serving_leg(args, C, rank):
@@ -661,8 +840,10 @@ def serving_leg(args, C, rank):
                       "served_vs_plain_windows_per_s": served["windows_per_s"] / plain["windows_per_s"],
                       "p99_served_le_plain": served["p99_ms"] <= plain["p99_ms"]})
         time.sleep(0.05)
+    parity = serving_parity(args, C, srv, tids, trees, built, reqs) if args.parity else None
     srv.close()
-    return {"workload": f"trees {args.serve_trees} uniform boxes, fanout {args.fanout}; "
+    return {"parity": parity,
+            "workload": f"trees {args.serve_trees} uniform boxes, fanout {args.fanout}; "
                         f"{len(reqs)} requests, Poisson arrivals, batch "
                         f"log-U[1, {args.serve_max_batch}] windows, side log-U[1e-5, 1e-1]",
             "windows": int(total_windows), "pairs": int(sum(stats)), "rates": rates}
@@ -685,7 +866,6 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     b = D.road_boxes(args.adv_boxes, seed=5 + 1000 * rank)
     q = D.road_windows(args.adv_windows, seed=105 + 1000 * rank)
     d = C.BBox.from_host(b)
-    del b
     rt = C.RTree(args.fanout)
     C.build_rtree(d, rt)
     dq = C.BBox.from_host(q)
@@ -708,6 +888,17 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     batched = {"windows_per_s": world * q.n / (ms / 1e3), "pairs_per_s": world * total / (ms / 1e3),
                "ms": ms, "pairs": int(total), "batches": st["batches"], "retries": st["retries"],
                "output_buffer_pairs": int(cap)}
+    # parity (untimed): the first windows (an i.i.d. sample of the mix) streamed
+    # again with their pairs digested on the device
+    m = min(q.n, max(0, args.parity_adv_windows)) if args.parity else 0
+    adv_digest = None
+    if m:
+        dg = C.PairDigest(m)
+        head = C.BBox(dq.xmin[:m], dq.ymin[:m], dq.xmax[:m], dq.ymax[:m], dq.id[:m])
+        sp = C.query_stream(rt, d, head, lambda f, t, a: dg.add(f, t, window_base=a),
+                            capacity=cap, batch=1 << 16)
+        adv_digest = dg.to_host() + (sp,)
+        del dg
 
     # served
     nserve = q.n // 10
@@ -721,35 +912,20 @@ def adversarial_leg(args, C, stream, dist, world, rank):
     tree = srv.add_tree(rt, d)
     windows = [C.BBox(dq.xmin[a:e], dq.ymin[a:e], dq.xmax[a:e], dq.ymax[a:e], dq.id[a:e])
                for a, e in reqs]
-    lat = np.zeros(len(reqs))
-    backlog, ids = [], {}
-    nxt = done = 0
-    pairs = retries = 0
-    t0 = time.monotonic()
-    while done < len(reqs):
-        now = time.monotonic() - t0
-        if now > SERVE_DEADLINE_S:
-            raise RuntimeError(f"serving run passed {SERVE_DEADLINE_S} s: {done} of {len(reqs)} done")
-        while nxt < len(reqs) and arrivals[nxt] <= now:
-            backlog.append(nxt)
-            nxt += 1
-        while backlog:
-            rid = srv.submit(tree, windows[backlog[0]])
-            if rid is None:
-                break
-            ids[rid] = backlog.pop(0)
-        for c in srv.poll(max_out=256, wait_ms=0 if (backlog or nxt < len(reqs)) else 2):
-            i = ids.pop(c["request_id"])
-            if c["status"] != 0:
-                raise RuntimeError(f"served request failed: {c}")
-            lat[i] = c["complete_time_s"] - (t0 + arrivals[i])
-            pairs += c["count"]
-            retries += c["retries"]
-            srv.release(c["request_id"])
-            done += 1
-        if nxt < len(reqs) and not backlog:
-            time.sleep(max(0.0, min(2e-4, arrivals[nxt] - (time.monotonic() - t0))))
-    span = time.monotonic() - t0
+    lat, span, pairs, retries = serve_run(srv, [tree], [(0, w) for w in windows], arrivals)
+    # parity replay (untimed): the requests over the first windows again, as
+    # fast as they are admitted, each one's pairs digested on completion
+    served_dg = None
+    if m:
+        served_dg = C.PairDigest(nserve)
+        first = [i for i, (a, e) in enumerate(reqs) if a < m]
+
+        def digest(i, c):
+            served_dg.add_ptr(c["d_fid"], c["d_tid"], c["count"], window_base=reqs[first[i]][0])
+            torch.cuda.current_stream().synchronize()  # read before the release
+
+        serve_run(srv, [tree], [(0, windows[i]) for i in first], np.zeros(len(first)),
+                  on_done=digest)
     srv.close()
     served_total = C.query_stats(rt, d, C.BBox(dq.xmin[:nserve], dq.ymin[:nserve], dq.xmax[:nserve],
                                                  dq.ymax[:nserve], dq.id[:nserve]))["hits"]
@@ -758,11 +934,30 @@ def adversarial_leg(args, C, stream, dist, world, rank):
               "windows_per_s": nserve / span, "p50_ms": float(np.percentile(lat, 50) * 1e3),
               "p99_ms": float(np.percentile(lat, 99) * 1e3), "retries": int(retries),
               "rate_req_s": 1000.0}
+    parity = None
+    if m:
+        from oracle import oracle as O
+        t0p = time.perf_counter()
+        sb, tr, tree_ok = oracle_tree(b, args.fanout, rt, d)
+        want = O.tree_query_stats(tr, sb, q.take(np.arange(m)))
+        bc, bh, bbad, sp = adv_digest
+        batched_cmp = dict(compare_digests(bc, bh, want.counts, want.hashes),
+                           pairs_outside_windows=bbad, retries=sp["retries"], batches=sp["batches"])
+        sm = min(m, nserve)
+        sc, sh, sbad = served_dg.to_host()
+        served_cmp = dict(compare_digests(sc[:sm], sh[:sm], want.counts[:sm], want.hashes[:sm]),
+                          pairs_outside_windows=sbad)
+        parity = {"ok": bool(tree_ok and batched_cmp["digest_ok"] and served_cmp["digest_ok"]
+                             and bbad == 0 and sbad == 0),
+                  "tree_identical": tree_ok, "windows_checked": m,
+                  "batched": batched_cmp, "served": served_cmp,
+                  "sample": f"the first {m} windows (i.i.d. draws of the mix)",
+                  "seconds": time.perf_counter() - t0p}
     rt.free()
     return {"workload": f"{args.adv_boxes // 1_000_000}M road boxes (100 segments, Pareto sides "
                         f"capped at 0.5, aspect up to 1e4), {args.adv_windows // 1000}k windows "
                         f"(50% points, 40% small, 10% over 1% of the domain), fanout {args.fanout}",
-            "batched": batched, "served": served}
+            "batched": batched, "served": served, "parity": parity}
 
 
 def ingest_leg(args, C, L, stream):
@@ -908,6 +1103,61 @@ def ingest_leg(args, C, L, stream):
                         "crt_read_mbr_csv_device(path, n, r=0)"}
 
 
+def config1_leg(args, C, stream, reps=10):
+    """The reference's own small case: 1M uniform boxes (side U[0,1e-3]),
+    10k windows (side U[0,1e-2]), fanout 10, through the drop-in calls a
+    reference caller makes (crt_build_f32 in place, crt_query_f32 allocating
+    the pairs), median of `reps` calls each; every window's pairs checked
+    against the reference's own brute force (nested_loop_query), as the
+    reference's driver checks them (src/rtree_test_frontier.cu:97-123)."""
+    import torch
+
+    from curtree_b200 import datasets as D
+    b = D.uniform_boxes(1_000_000, seed=1)
+    q = D.uniform_windows(10_000, seed=101)
+    bms, qms = [], []
+    dg = None
+    for r in range(reps + 1):
+        d = C.BBox.from_host(b)
+        rt = C.RTree(10)
+        dq = C.BBox.from_host(q)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        C.build_rtree(d, rt, stream)
+        e1.record(stream)
+        e1.synchronize()
+        b_ms = e0.elapsed_time(e1)
+        e0.record(stream)
+        pr = C.bfs_frontier(rt, d, dq, stream)
+        e1.record(stream)
+        e1.synchronize()
+        if r:  # the first call of each is a warm-up
+            bms.append(b_ms)
+            qms.append(e0.elapsed_time(e1))
+        if r == reps and args.parity:
+            dg = C.PairDigest(q.n)
+            dg.add_ptr(pr.s.fid, pr.s.tid, pr.sz)
+            dg = dg.to_host()
+        npairs = pr.sz
+        pr.free()
+        rt.free()
+        del d, dq
+    out = {"workload": "1M uniform boxes (side U[0,1e-3]) x 10k windows (side U[0,1e-2]), "
+                       "fanout 10; crt_build_f32 + crt_query_f32 (drop-in)",
+           "build_ms": statistics.median(bms), "query_ms": statistics.median(qms),
+           "pairs": int(npairs), "calls": reps}
+    if dg is not None:
+        from oracle import oracle as O
+        if O.ref_cpu_available():
+            c, h, n, secs = O.ref_nested_loop_digest(q, b, np.arange(q.n, dtype=np.int32))
+            cmp = compare_digests(dg[0], dg[1], c, h)
+            out["parity"] = dict(cmp, ok=bool(cmp["digest_ok"] and dg[2] == 0),
+                                 against="the reference's nested_loop_query on every window "
+                                         f"({secs:.1f} s on {os.cpu_count()} host threads)")
+    return out
+
+
 def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
     import torch
     from curtree_b200 import datasets as D
@@ -938,11 +1188,30 @@ def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
     profile_collect(None)
     L.crt_profile_enable(0)
     ms = reduce_max(ms, dist)
+    # the drop-in call as the reference's build_rtree is called (crt_build_f32:
+    # in place, allocates the node arrays), on a fresh copy of the input each time
+    work = C.BBox.empty(n)
+    dms = []
+    for _ in range(3):
+        for dst, src in zip((work.xmin, work.ymin, work.xmax, work.ymax, work.id),
+                            (d_in.xmin, d_in.ymin, d_in.xmax, d_in.ymax, d_in.id)):
+            dst.copy_(src)
+        rt2 = C.RTree(f)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        C.build_rtree(work, rt2, stream)
+        e1.record(stream)
+        e1.synchronize()
+        dms.append(e0.elapsed_time(e1))
+        rt2.free()
+    del work
     kern_ms = sum(parts.values())
     b_build = 120 * n + 40 * rsz
     strict = 40 * n + 24 * rsz
     return {"metric": "build_boxes_per_s", "value": world * n / (ms / args.steps / 1e3),
             "unit": "boxes/s", "ms_per_step": ms / args.steps, "kernel_ms": kern_ms,
+            "dropin_ms": statistics.median(dms),
             "kernels_ms": parts, "fanout": f, "boxes": n, "r_sz": rsz,
             "workload": "100M clustered boxes (1000 Gaussians + 10% uniform, log-normal sides, "
                         "1% duplicates, 1% points), out-of-place crt_build_into_f32",
@@ -952,6 +1221,66 @@ def build_leg(args, C, L, hbm_peak, peak_kind, stream, dist, world):
                          "peak_kind": peak_kind, "algorithmic_bytes": b_build,
                          "bytes_model": "120 B/box + 40 B/node",
                          "strict_io_frac": strict / (kern_ms / 1e3) / 1e9 / hbm_peak}}
+
+
+def reference_gpu_leg():
+    """The reference's own GPU path (build_rtree + bfs_frontier compiled from
+    its sources into oracle/_ref/ref_frontier, sm_100) on this GPU, timed
+    with CUDA events by the runner: its small case (1M boxes x 10k windows),
+    the 100M clustered build, and the 10M-box x 1M-window batch of this
+    benchmark's headline, on which it stops at its frontier-queue limit."""
+    import shutil
+
+    from curtree_b200 import datasets as D
+    from oracle import ref_gpu as R
+    if not R.available("ref_frontier"):
+        return {"unavailable": "oracle/_ref/ref_frontier was not built (the reference sources "
+                               "were absent when build() ran)"}
+    out = {"runner": "oracle/_ref/ref_frontier: the reference's build_rtree "
+                     "(src/rtree_bulkload_thrust.cuh:62) and bfs_frontier "
+                     "(src/rtree_bfs_frontier.cuh:292), unchanged, CUDA-event timed"}
+    tmp = tempfile.mkdtemp(prefix="crt_ref_")
+    try:
+        cases = [("small", lambda: D.uniform_boxes(1_000_000, seed=1),
+                  lambda b: D.uniform_windows(10_000, seed=101), 10, 5),
+                 ("build_100M_clustered", lambda: D.clustered_boxes(100_000_000, seed=2),
+                  None, 10, 3),
+                 ("batched_10M_x_1M", lambda: D.uniform_boxes(10_000_000, seed=3),
+                  lambda b: D.mixed_windows(1_000_000, b, seed=103), 10, 1)]
+        for name, mk_b, mk_q, f, reps in cases:
+            b = mk_b()
+            bfile = os.path.join(tmp, name + "_b.crtb")
+            b.write_crtb(bfile)
+            qfile = None
+            if mk_q is not None:
+                q = mk_q(b)
+                qfile = os.path.join(tmp, name + "_q.crtb")
+                q.write_crtb(qfile)
+                del q
+            nb = b.n
+            del b
+            t0 = time.perf_counter()
+            try:
+                _, _, pairs, info = R.run("ref_frontier", "query" if qfile else "build", bfile, qfile,
+                                          f, os.path.join(tmp, name), reps=reps, timeout=600,
+                                          want_pairs=False)
+                rec = {"boxes": nb, "fanout": f, "build_ms": statistics.median(info["build_ms"]),
+                       "build_boxes_per_s": nb / (statistics.median(info["build_ms"]) / 1e3)}
+                if info.get("query_ms"):
+                    rec["query_ms"] = statistics.median(info["query_ms"])
+                if "pairs" in info:
+                    rec["pairs"] = info["pairs"]
+            except R.RefRunFailed as e:
+                tail = [ln for ln in (e.stdout + e.stderr).splitlines() if ln.strip()][-2:]
+                rec = {"boxes": nb, "fanout": f, "failed": f"exit {e.rc}", "output_tail": tail}
+            rec["wall_s"] = time.perf_counter() - t0
+            out[name] = rec
+            for x in os.listdir(tmp):
+                pth = os.path.join(tmp, x)
+                shutil.rmtree(pth) if os.path.isdir(pth) else os.remove(pth)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return out
 
 
 def main():
@@ -984,6 +1313,11 @@ def main():
                                  "kind": r["kind"], "sample": samples[-1]},
                 "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        if args.reference_gpu:
+            try:
+                line["reference_gpu"] = reference_gpu_leg()
+            except Exception as e:  # a side record: report it, keep the line
+                line["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"}
         print(json.dumps(line), flush=True)
         return
 
@@ -1000,9 +1334,29 @@ def main():
     skip = set(s for s in args.skip.split(",") if s)
     cpu = None
     if rank == 0 and world == 1 and "cpu" not in skip:
-        cpu = cpu_reference_rate(boxes, windows, args.cpu_seconds)
+        cpu, (idx, rc, rh) = cpu_reference_rate(boxes, windows, args.cpu_seconds, keep=True)
+        dg = out.pop("_digests", {})
+        if rh is not None and "persistent" in dg and out.get("parity"):
+            c, h, _ = dg["persistent"]
+            cmp = compare_digests(c[idx], h[idx], rc, rh)
+            out["parity"]["reference_brute_force"] = dict(
+                cmp, what="the reference's own nested_loop_query (src/utility.h:22-45, compiled "
+                          "from its sources) on the CPU baseline's sample, against the persistent "
+                          "form's digests")
+            out["parity"]["ok"] = bool(out["parity"]["ok"] and cmp["digest_ok"])
+    out.pop("_digests", None)
     if rank == 0:
         p = out["persistent"]
+        detail = {"persistent": p, "plain": out.get("plain"), "build": out.get("build"),
+                  "serving": out.get("serving"), "adversarial": out.get("adversarial"),
+                  "ingest": out.get("ingest"), "cpu_rtree": out.get("cpu_rtree"),
+                  "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
+                  "parity": out.get("parity"), "e2e": out.get("e2e"), "roofline": out["roofline"],
+                  "config1": out.get("config1")}
+        if args.detail:
+            with open(args.detail, "w") as f:
+                json.dump(detail, f, indent=1)
+        print("detail: " + json.dumps(detail), file=sys.stderr, flush=True)
         line = {"metric": "window_queries_per_s", "value": p["windows_per_s"], "unit": "windows/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": p["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -1010,17 +1364,101 @@ def main():
                 "config": query_config(args),
                 "roofline": out["roofline"], "cpu_baseline": cpu, "e2e": out.get("e2e"),
                 "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
-                "plain": out.get("plain"), "build": out.get("build"),
-                "serving": out.get("serving"), "adversarial": out.get("adversarial"),
-                "ingest": out.get("ingest"), "cpu_rtree": out.get("cpu_rtree"),
-                "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                 "persistent_kernel_ms": p["kernel_ms"]}
+        line.update(compact_legs(out))
         if "plain" in out:
             line["persistent_vs_plain"] = p["windows_per_s"] / out["plain"]["windows_per_s"]
+            line["batch_latency_ms"] = {
+                "persistent": {k: round(v, 3) for k, v in p["batch_latency"].items()},
+                "plain": {k: round(v, 3) for k, v in out["plain"]["batch_latency"].items()}}
+        line["parity"] = compact_parity(out)
         print(json.dumps(line), flush=True)
+        failed = [k for k, v in line["parity"].items() if isinstance(v, dict) and v.get("ok") is False]
+        if failed:
+            print(f"parity FAILED: {failed}", file=sys.stderr, flush=True)
+            sys.exit(3)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _r(x, nd=3):
+    return None if x is None else round(float(x), nd)
+
+
+def compact_legs(out):
+    """The sub-legs in a few keys each, so the end of the line carries them;
+    the full figures go to the detail record."""
+    o = {}
+    if out.get("cpu_rtree") and "value" in out["cpu_rtree"]:
+        o["cpu_rtree_windows_per_s"] = _r(out["cpu_rtree"]["value"], 1)
+    a = out.get("autotune")
+    if a:
+        o["autotune"] = {"chosen": a["chosen"], "rows": len(a["table"]),
+                         "sample_windows": a["sample_windows"]}
+    g = out.get("ingest")
+    if g:
+        o["ingest"] = {"records_per_s": _r(g["value"], 0), "ms": _r(g["ms_per_step"]),
+                       "gpu_kernels_ms": _r(g["gpu_kernels_ms"]),
+                       "speedup_vs_host_loader": _r(g["speedup_vs_host_loader"], 1),
+                       "identical_to_host_loader": g["identical_to_host_loader"],
+                       "binary_records_per_s": _r(g["binary"]["records_per_s"], 0)}
+    v = out.get("adversarial")
+    if v:
+        b, sv = v["batched"], v["served"]
+        o["adversarial"] = {"batched_pairs_per_s": _r(b["pairs_per_s"], 0), "batched_ms": _r(b["ms"], 1),
+                            "pairs": b["pairs"], "retries": b["retries"],
+                            "served_p50_ms": _r(sv["p50_ms"], 2), "served_p99_ms": _r(sv["p99_ms"], 2),
+                            "served_retries": sv["retries"]}
+    sv = out.get("serving")
+    if sv:
+        o["serving"] = [{"rate": int(r["rate_req_s"]), "served_wps": _r(r["served"]["windows_per_s"], 0),
+                         "plain_wps": _r(r["plain"]["windows_per_s"], 0),
+                         "ratio": _r(r["served_vs_plain_windows_per_s"], 2),
+                         "p99_ms": [_r(r["served"]["p99_ms"], 1), _r(r["plain"]["p99_ms"], 1)]}
+                        for r in sv["rates"]]
+    if out.get("plain"):
+        o["plain_windows_per_s"] = _r(out["plain"]["windows_per_s"], 0)
+    c1 = out.get("config1")
+    if c1:
+        o["config1"] = {"build_ms": _r(c1["build_ms"]), "query_ms": _r(c1["query_ms"]),
+                        "pairs": c1["pairs"]}
+    bd = out.get("build")
+    if bd:
+        o["build"] = {"boxes_per_s": _r(bd["value"], 0), "ms_per_step": _r(bd["ms_per_step"]),
+                      "dropin_ms": _r(bd["dropin_ms"]),
+                      "kernels_ms": {k: _r(x) for k, x in bd["kernels_ms"].items()},
+                      "roofline_frac": _r(bd["roofline"]["frac"]),
+                      "strict_io_frac": _r(bd["roofline"]["strict_io_frac"])}
+    return o
+
+
+def compact_parity(out):
+    p = {}
+    h = out.get("parity")
+    if h:
+        p["headline"] = {"ok": h["ok"], "tree_identical": h["tree_identical"],
+                         "windows_checked": h["windows_checked"], "pairs_checked": h["pairs_checked"],
+                         "forms_digest_ok": {k: f["digest_ok"] for k, f in h["forms"].items()}}
+        rb = h.get("reference_brute_force")
+        if rb:
+            p["reference_brute_force"] = {"ok": rb["digest_ok"], "windows": rb["windows"],
+                                          "pairs": rb["pairs"]}
+    c1 = (out.get("config1") or {}).get("parity")
+    if c1:
+        p["config1"] = {"ok": c1["ok"], "windows": c1["windows"], "pairs": c1["pairs"]}
+    v = (out.get("adversarial") or {}).get("parity")
+    if v:
+        p["adversarial"] = {"ok": v["ok"], "tree_identical": v["tree_identical"],
+                            "windows_checked": v["windows_checked"],
+                            "pairs_checked": v["batched"]["pairs"],
+                            "batched_ok": v["batched"]["digest_ok"], "served_ok": v["served"]["digest_ok"]}
+    sv = (out.get("serving") or {}).get("parity")
+    if sv:
+        p["serving"] = {"ok": sv["ok"], "trees_identical": sv["trees_identical"],
+                        "requests_checked": sv["requests_checked"],
+                        "windows_checked": sv["windows_checked"], "pairs_checked": sv["pairs_checked"]}
+    return p
 
 
 def query_config(args):

@@ -112,6 +112,7 @@ SIGNATURES = {
                                           ctypes.POINTER(crt_query_opts), _vp]),
     "crt_query_capacity": (_i64, [_i64, ctypes.POINTER(crt_query_opts)]),
     "crt_pairs_canonicalize": (ctypes.c_int, [_vp, _vp, _i64, _vp]),
+    "crt_pairs_digest": (ctypes.c_int, [_vp, _vp, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
     "crt_read_mbr_csv": (ctypes.c_int, [ctypes.c_char_p, _i64, ctypes.c_float, _vp, _vp, _vp, _vp,
                                         _vp, ctypes.POINTER(_i64)]),
     "crt_read_mbr_csv_device": (ctypes.c_int, [ctypes.c_char_p, _i64, ctypes.c_float,

@@ -368,6 +368,14 @@ int crt_pairs_canonicalize(int32_t* d_fid, int32_t* d_tid, int64_t n, crt_stream
   return pairs_canonicalize(d_fid, d_tid, n, (cudaStream_t)stream);
 }
 
+int crt_pairs_digest(const int32_t* d_fid, const int32_t* d_tid, int64_t n, int64_t window_base,
+                     int64_t nq, int64_t* d_counts, uint64_t* d_hashes, int64_t* d_bad,
+                     crt_stream_t stream)
+{
+  return pairs_digest(d_fid, d_tid, n, window_base, nq, d_counts, d_hashes, d_bad,
+                      (cudaStream_t)stream);
+}
+
 int crt_query_plain_noalloc_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
                                 const crt_bbox_f32* d_qbox, int32_t* d_fid, int32_t* d_tid,
                                 int64_t capacity, crt_query_result* d_result, crt_stream_t stream)

@@ -616,6 +616,7 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
                float* nymin, float* nxmax, float* nymax, int* npos, int* nlen,
                cudaStream_t stream)
 {
+  NvtxRange range("crt_build");
   std::vector<int64_t> lv;
   if (tree_levels(n, fanout, lv) < 0)
     return fail(CRT_ERR_INVALID_ARG, "build: need n >= 1 and fanout >= 2");

@@ -91,4 +91,101 @@ int pairs_canonicalize(int32_t* fid, int32_t* tid, int64_t n, cudaStream_t strea
   return CRT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Per-window counts and order-independent digests of a pair list.  The
+// reference's drivers check a result by sorting both pair vectors and
+// comparing them (src/rtree_test_frontier.cu:102-123); at billions of pairs
+// the same check is a per-window count plus a per-window sum (mod 2^64) of a
+// 64-bit mix of each (window, box id) pair, which any pair order gives alike.
+// The mix is the splitmix64 finaliser (Steele, Lea and Flood, "Fast
+// splittable pseudorandom number generators", OOPSLA 2014).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long pair_mix(unsigned long long z)
+{
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+constexpr int kDigestRun = 64;  // consecutive pairs per thread
+
+// Each thread sums the pairs of its run window by window and adds each
+// window's count and digest with one pair of atomics; when every lane of a
+// warp saw one window only (the long runs of a batch query's output), the
+// warp adds once.
+__global__ void __launch_bounds__(256)
+    digest_kernel(const int32_t* __restrict__ fid, const int32_t* __restrict__ tid, int64_t n,
+                  int64_t base, int64_t nq, unsigned long long* __restrict__ counts,
+                  unsigned long long* __restrict__ hashes, unsigned long long* __restrict__ bad)
+{
+  const int64_t nruns = (n + kDigestRun - 1) / kDigestRun;
+  for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x; r0 < nruns;
+       r0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = r0 + threadIdx.x;
+    const int64_t i0 = r * kDigestRun;
+    const int64_t i1 = min(n, i0 + kDigestRun);
+    long long cur = -1;  // window of the open segment
+    unsigned long long c = 0, h = 0, nbad = 0;
+    bool single = true;  // the whole run is one window
+    for (int64_t i = i0; i < i1; i++) {
+      const long long w = (long long)__ldg(tid + i) + base;
+      if (w < 0 || w >= nq) {
+        nbad++;
+        single = false;
+        continue;
+      }
+      if (w != cur) {
+        if (cur >= 0) {
+          atomicAdd(&counts[cur], c);
+          atomicAdd(&hashes[cur], h);
+          single = false;
+        }
+        cur = w;
+        c = 0;
+        h = 0;
+      }
+      c++;
+      h += pair_mix(((unsigned long long)(uint32_t)w << 32) | (uint32_t)__ldg(fid + i));
+    }
+    // warp aggregation: all lanes hold one segment of the same window
+    const long long w0 = __shfl_sync(0xffffffffu, cur, 0);
+    const bool same = __all_sync(0xffffffffu, single && cur == w0 && cur >= 0);
+    if (same) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, o);
+        h += __shfl_down_sync(0xffffffffu, h, o);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&counts[w0], c);
+        atomicAdd(&hashes[w0], h);
+      }
+    } else if (cur >= 0) {
+      atomicAdd(&counts[cur], c);
+      atomicAdd(&hashes[cur], h);
+    }
+    if (nbad && bad) atomicAdd(bad, nbad);
+  }
+}
+
+int pairs_digest(const int32_t* fid, const int32_t* tid, int64_t n, int64_t window_base,
+                 int64_t nq, int64_t* d_counts, uint64_t* d_hashes, int64_t* d_bad,
+                 cudaStream_t stream)
+{
+  if (n < 0 || nq < 0 || (n > 0 && (!fid || !tid)) || (nq > 0 && (!d_counts || !d_hashes)))
+    return fail(CRT_ERR_INVALID_ARG, "pairs_digest: bad arguments");
+  if (n == 0) return CRT_OK;
+  const int64_t nruns = cdiv(n, kDigestRun);
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(nruns, 256), (int64_t)sm_count() * 8));
+  digest_kernel<<<grid, 256, 0, stream>>>(fid, tid, n, window_base, nq,
+                                          (unsigned long long*)d_counts,
+                                          (unsigned long long*)d_hashes,
+                                          (unsigned long long*)d_bad);
+  CRT_LAUNCHED(1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "pairs_digest");
+  return CRT_OK;
+}
+
 }  // namespace crt

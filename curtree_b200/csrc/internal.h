@@ -53,6 +53,9 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
                cudaStream_t stream);
 
 int pairs_canonicalize(int32_t* fid, int32_t* tid, int64_t n, cudaStream_t stream);
+int pairs_digest(const int32_t* fid, const int32_t* tid, int64_t n, int64_t window_base,
+                 int64_t nq, int64_t* d_counts, uint64_t* d_hashes, int64_t* d_bad,
+                 cudaStream_t stream);
 
 // Query entry used by the C ABI.
 int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,

@@ -47,6 +47,23 @@ void prof_stop(int token, cudaStream_t stream)
   if (token < (int)g_recs.size()) cudaEventRecord(g_recs[token].b, stream);
 }
 
+bool prof_register(const char* name, cudaEvent_t* a, cudaEvent_t* b)
+{
+  if (!g_on) return false;
+  Rec r;
+  r.name = name;
+  if (cudaEventCreate(&r.a) != cudaSuccess) return false;
+  if (cudaEventCreate(&r.b) != cudaSuccess) {
+    cudaEventDestroy(r.a);
+    return false;
+  }
+  *a = r.a;
+  *b = r.b;
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_recs.push_back(r);
+  return true;
+}
+
 void prof_add(const char* name, double ms)
 {
   std::lock_guard<std::mutex> lk(g_mu);

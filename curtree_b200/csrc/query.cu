@@ -803,18 +803,30 @@ LevelTables level_tables(const crt_rtree_f32& rt, int64_t nbox)
   return t;
 }
 
-// Uploads the tables to `dev` (kLevelTableBytes, 8-byte aligned) and points
-// the view at them.
+// Writes the tables (passed by value) to device memory: a one-thread kernel
+// instead of a copy from host memory, so the caller's host thread never waits
+// on a pageable transfer and the write can be recorded in a CUDA graph.
+__global__ void write_levels_kernel(LevelTables t, int* __restrict__ first,
+                                    long long* __restrict__ span)
+{
+  for (int h = threadIdx.x; h < kMaxLevels; h += blockDim.x) {
+    first[h] = t.first[h];
+    span[h] = t.span[h];
+  }
+}
+
+// Puts the tables at `dev` (kLevelTableBytes, 8-byte aligned) and points the
+// view at them.
 static void attach_levels(TreeView& T, const LevelTables& t, void* dev, cudaStream_t stream)
 {
   if (t.nlev == 0) return;
-  char buf[kLevelTableBytes];
-  std::memcpy(buf, t.first, sizeof(int) * kMaxLevels);
-  std::memcpy(buf + sizeof(int) * kMaxLevels, t.span, sizeof(long long) * kMaxLevels);
-  cudaMemcpyAsync(dev, buf, kLevelTableBytes, cudaMemcpyHostToDevice, stream);
+  int* first = (int*)dev;
+  long long* span = (long long*)((char*)dev + sizeof(int) * kMaxLevels);
+  write_levels_kernel<<<1, 64, 0, stream>>>(t, first, span);
+  CRT_LAUNCHED(1);
   T.nlev = t.nlev;
-  T.lvl_first = (const int*)dev;
-  T.lvl_span = (const long long*)((char*)dev + sizeof(int) * kMaxLevels);
+  T.lvl_first = first;
+  T.lvl_span = span;
 }
 
 // Number of levels of a tree with R_sz nodes over nbox boxes at this fanout
@@ -955,8 +967,7 @@ static void persist_scratch_carve(char* base, int64_t max_nq, long long max_hole
 // A persistent query is three stages on one stream, none synchronising the
 // host: `pre` (reset the counters, order the windows), the traversal kernel,
 // and `post` (sort the unused chunk ends, compact, write the result block).
-// The plan records pre and post as CUDA graphs and launches the traversal
-// between them, so its duration can be taken with ordinary events.
+// A plan records all three as one CUDA graph.
 static void enqueue_pre(const WindowView& W, int64_t max_nq, const PersistScratch& S, bool sort,
                         cudaStream_t stream)
 {
@@ -1013,12 +1024,13 @@ static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
   return L;
 }
 
-static void launch_traverse(const TraverseLaunch& L, cudaStream_t stream)
+static cudaError_t launch_traverse(const TraverseLaunch& L, cudaStream_t stream)
 {
   ProfScope ps("traverse_persistent", stream);
   void* args[] = {(void*)&L.P};
-  cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.threads), args, L.smem, stream);
+  cudaError_t e = cudaLaunchKernel(L.fn, dim3(L.grid), dim3(L.threads), args, L.smem, stream);
   CRT_LAUNCHED(1);
+  return e;
 }
 
 static void enqueue_post(const PersistScratch& S, int32_t* fid, int32_t* tid, long long cap,
@@ -1054,6 +1066,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
                int32_t* fid, int32_t* tid, int64_t capacity, crt_query_result* d_result,
                int64_t* d_offsets, const crt_query_opts& opts, cudaStream_t stream)
 {
+  NvtxRange range(opts.mode == CRT_QUERY_PLAIN ? "crt_query_plain" : "crt_query_persistent");
   if (!d_result) return fail(CRT_ERR_INVALID_ARG, "query: result block is required");
   if (qbox.sz < 0 || rbox.sz < 0 || rt.sz < 0)
     return fail(CRT_ERR_INVALID_ARG, "query: negative size");
@@ -1134,12 +1147,13 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   set_nq_kernel<<<1, 1, 0, stream>>>(S.ctr, nq);
   CRT_LAUNCHED(1);
   enqueue_pre(W, nq, S, sort, stream);
-  launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk,
-                                opts.warps_per_cta),
-                  stream);
+  cudaError_t e = launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk,
+                                                opts.warps_per_cta),
+                                  stream);
   enqueue_post(S, fid, tid, capacity, d_result, stream);
   cudaFreeAsync(scr, stream);
-  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  else cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "query (persistent)");
   (void)sms;
   return CRT_OK;
@@ -1295,6 +1309,12 @@ int query_stats(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
 // ---------------------------------------------------------------------------
 // Persistent plan captured in a CUDA graph
 // ---------------------------------------------------------------------------
+// The whole query -- counter reset, window ordering, the persistent traversal
+// and the output compaction -- is one graph, replayed with one
+// cudaGraphLaunch.  Two event-record nodes bracket the traversal: they record
+// the plan's own events, or, while kernel timing is on, a fresh event pair
+// per launch (set into the instantiated graph before the launch), so the
+// traversal's duration is measured inside the replay.
 struct Plan {
   TreeView T;
   WindowView W;
@@ -1309,11 +1329,30 @@ struct Plan {
   long long cap;
   crt_query_result* res;
   TraverseLaunch traverse;
-  cudaGraph_t graph[2] = {nullptr, nullptr};  // pre, post
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t own[2] = {nullptr, nullptr};         // recorded when timing is off
+  cudaGraphNode_t ev_node[2] = {nullptr, nullptr};  // the event-record nodes
 };
 
 int plan_destroy(void* hp);
+
+// The event-record node of `graph` that records `ev`.
+static cudaGraphNode_t find_event_node(cudaGraph_t graph, cudaEvent_t ev)
+{
+  size_t n = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess || n == 0) return nullptr;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return nullptr;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    cudaEvent_t e = nullptr;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeEventRecord &&
+        cudaGraphEventRecordNodeGetEvent(nd, &e) == cudaSuccess && e == ev)
+      return nd;
+  }
+  return nullptr;
+}
 
 int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
                 int64_t max_nq, int32_t* fid, int32_t* tid, int64_t capacity,
@@ -1348,32 +1387,37 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   if (!opts.no_contain) attach_levels(p->T, level_tables(rt, rbox.sz), p->scratch + p->S.bytes, stream);
   cudaMemsetAsync(p->S.ctr, 0, sizeof(QueryCounters), stream);
   set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
+  CRT_LAUNCHED(1);
   p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk,
                               opts.warps_per_cta);
-  // capture pre and post on a private stream
-  cudaStream_t cs;
-  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
-    cudaFree(p->scratch);
-    delete p;
-    return cuda_fail(cudaGetLastError(), "plan: stream");
+  // capture the whole query on a private stream; a window-sorting plan
+  // orders exactly max_nq windows, so it only runs with nq == max_nq
+  // (plan_set_nq enforces it); without sorting the kernel reads the live
+  // count from ctr->nq
+  cudaStream_t cs = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&p->own[0]);
+  if (e == cudaSuccess) e = cudaEventCreate(&p->own[1]);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue_pre(p->W, max_nq, p->S, p->sort, cs);
+    cudaError_t le = cudaEventRecordWithFlags(p->own[0], cs, cudaEventRecordExternal);
+    if (le == cudaSuccess) le = launch_traverse(p->traverse, cs);
+    if (le == cudaSuccess) le = cudaEventRecordWithFlags(p->own[1], cs, cudaEventRecordExternal);
+    enqueue_post(p->S, fid, tid, capacity, res, cs);
+    e = cudaStreamEndCapture(cs, &p->graph);
+    if (e == cudaSuccess && le != cudaSuccess) e = le;
   }
-  // a window-sorting plan orders exactly max_nq windows, so it only runs with
-  // nq == max_nq (plan_set_nq enforces it); without sorting the kernel reads
-  // the live count from ctr->nq
-  cudaError_t e = cudaSuccess;
-  for (int g = 0; g < 2 && e == cudaSuccess; g++) {
-    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) break;
-    if (g == 0)
-      enqueue_pre(p->W, max_nq, p->S, p->sort, cs);
-    else
-      enqueue_post(p->S, fid, tid, capacity, res, cs);
-    e = cudaStreamEndCapture(cs, &p->graph[g]);
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec[g], p->graph[g], 0);
+  if (e == cudaSuccess) {
+    p->ev_node[0] = find_event_node(p->graph, p->own[0]);
+    p->ev_node[1] = find_event_node(p->graph, p->own[1]);
+    if (!p->ev_node[0] || !p->ev_node[1]) e = cudaErrorInvalidValue;
   }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
   cudaStreamSynchronize(stream);
-  cudaStreamDestroy(cs);
+  if (cs) cudaStreamDestroy(cs);
   if (e != cudaSuccess) {
+    cudaGetLastError();
     plan_destroy(p);
     return cuda_fail(e, "plan: graph capture");
   }
@@ -1395,14 +1439,17 @@ int plan_set_nq(void* hp, int64_t nq, cudaStream_t stream)
 
 int plan_launch(void* hp, cudaStream_t stream)
 {
+  NvtxRange range("crt_plan_launch");
   Plan* p = (Plan*)hp;
-  cudaError_t e = cudaGraphLaunch(p->exec[0], stream);
+  cudaEvent_t a = p->own[0], b = p->own[1];
+  prof_register("traverse_persistent", &a, &b);  // leaves the plan's own pair when off
+  cudaError_t e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[0], a);
+  if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[1], b);
+  if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, stream);
   if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
-  CRT_LAUNCHED(p->sort ? 6 : 0);  // window keys, sort plan, four sort passes
-  launch_traverse(p->traverse, stream);
-  e = cudaGraphLaunch(p->exec[1], stream);
-  CRT_LAUNCHED(3);
-  if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
+  // window keys, sort plan, four sort passes; the traversal; hole sort,
+  // prefix and compaction
+  CRT_LAUNCHED((p->sort ? 6 : 0) + 1 + 3);
   return CRT_OK;
 }
 
@@ -1410,10 +1457,10 @@ int plan_destroy(void* hp)
 {
   Plan* p = (Plan*)hp;
   if (!p) return CRT_OK;
-  for (int g = 0; g < 2; g++) {
-    if (p->exec[g]) cudaGraphExecDestroy(p->exec[g]);
-    if (p->graph[g]) cudaGraphDestroy(p->graph[g]);
-  }
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  for (auto ev : p->own)
+    if (ev) cudaEventDestroy(ev);
   if (p->scratch) cudaFree(p->scratch);
   delete p;
   return CRT_OK;

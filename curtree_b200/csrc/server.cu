@@ -33,6 +33,7 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -300,6 +301,7 @@ class Arena {
   }
   void release(size_t off, size_t bytes)
   {
+    if (bytes == 0) return;
     bytes = (bytes + 255) / 256 * 256;
     used_ -= bytes;
     auto it = free_.emplace(off, bytes).first;
@@ -334,7 +336,11 @@ struct Request {
   double t_submit = 0;
   int retries = 0;
   double predicted = 0;  // area-based pair estimate (0: none)
+  // a re-run's windows, held on the host while it waits for arena space
+  std::shared_ptr<std::vector<float>> host_windows;
 };
+
+size_t granules(size_t bytes) { return (bytes + 255) / 256 * 256; }
 
 // Host-side statistics of a tree for output estimates.
 struct TreeStats {
@@ -499,8 +505,8 @@ struct Server {
     c.status = status;
     c.nq = q.nq;
     c.count = count;
-    c.d_fid = (int32_t*)(arena + q.out_off);
-    c.d_tid = c.d_fid + q.cap;
+    c.d_fid = q.out_bytes ? (int32_t*)(arena + q.out_off) : nullptr;
+    c.d_tid = q.out_bytes ? c.d_fid + q.cap : nullptr;
     c.submit_time_s = q.t_submit;
     c.complete_time_s = now_s();
     c.retries = q.retries;
@@ -523,20 +529,32 @@ struct Server {
           progressed = true;
           learn_locked(q, count);
           if (count > q.cap) {
-            // overflow-and-retry: re-run with the exact size once the arena
-            // has room for it
+            // overflow-and-retry: re-run with the exact size.  The windows
+            // move to the host and both of the request's blocks are freed,
+            // so the re-run needs one block (windows + exact output) that
+            // fits as soon as the arena drains: waiting for an output block
+            // beside a window block left in the middle of the arena could
+            // wait forever.
             n_retried++;
-            alloc.release(q.out_off, q.out_bytes);
             Request rq = q;
+            rq.host_windows = std::make_shared<std::vector<float>>((size_t)q.nq * 4);
+            cudaError_t ce = cudaMemcpyAsync(rq.host_windows->data(), arena + q.win_off,
+                                             (size_t)q.nq * 16, cudaMemcpyDeviceToHost, copy);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(copy);
+            alloc.release(q.out_off, q.out_bytes);
+            alloc.release(q.win_off, q.win_bytes);
             rq.cap = count;
             rq.out_bytes = (size_t)count * 8;
-            rq.out_off = 0;
+            rq.win_off = rq.out_off = 0;
             rq.retries++;
             rq.seq = -1;
-            if (rq.out_bytes + rq.win_bytes > arena_bytes) {
-              rq.out_bytes = 0;
+            if (ce != cudaSuccess || granules(rq.win_bytes) + granules(rq.out_bytes) > arena_bytes) {
+              // never fits (or the windows could not be saved): fail it
+              if (ce != cudaSuccess) cudaGetLastError();
+              rq.win_bytes = rq.out_bytes = 0;
               rq.cap = 0;
-              finish_locked(rq, count, CRT_ERR_OOM);
+              rq.host_windows.reset();
+              finish_locked(rq, count, ce != cudaSuccess ? CRT_ERR_CUDA : CRT_ERR_OOM);
             } else {
               retry_wait.push_back(rq);
             }
@@ -555,13 +573,26 @@ struct Server {
       } else {
         oldest_seq = next_seq;
       }
-      // re-runs waiting for arena space, oldest first
+      // re-runs waiting for arena space, oldest first: one block holds the
+      // windows (copied back in) and the exact output
       while (!retry_wait.empty()) {
+        Request& f = retry_wait.front();
         size_t off;
-        if (!alloc.alloc(retry_wait.front().out_bytes, off)) break;
-        Request rq = retry_wait.front();
+        if (!alloc.alloc(granules(f.win_bytes) + granules(f.out_bytes), off)) break;
+        Request rq = f;
         retry_wait.pop_front();
-        rq.out_off = off;
+        rq.win_off = off;
+        rq.out_off = off + granules(rq.win_bytes);
+        cudaError_t ce = cudaMemcpyAsync(arena + rq.win_off, rq.host_windows->data(),
+                                         (size_t)rq.nq * 16, cudaMemcpyHostToDevice, copy);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(copy);
+        rq.host_windows.reset();
+        if (ce != cudaSuccess) {
+          cudaGetLastError();
+          finish_locked(rq, 0, CRT_ERR_CUDA);
+          progressed = true;
+          continue;
+        }
         pending.push_back(rq);
       }
       if (progressed) cv.notify_all();
@@ -571,7 +602,9 @@ struct Server {
         last_work = now_s();
       }
       if (!flight.empty()) last_work = now_s();
-      if (kernel_running && flight.empty() && pending.empty() && retry_wait.empty() &&
+      // re-runs waiting for space do not keep the device loop running: their
+      // space comes from requests the client releases, not from the device
+      if (kernel_running && flight.empty() && pending.empty() &&
           now_s() - last_work > opts.idle_ms * 1e-3) {
         lk.unlock();
         stop_kernel();
@@ -777,6 +810,10 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
       return fail(CRT_ERR_INVALID_ARG, "server_submit: unknown tree");
     if ((long long)(s->flight.size() + s->pending.size()) >= s->slots)
       return fail(CRT_ERR_BUSY, "server_submit: all request slots in use");
+    // a re-run waiting for arena space goes first: new requests would take
+    // the space it waits for
+    if (!s->retry_wait.empty())
+      return fail(CRT_ERR_BUSY, "server_submit: a re-run is waiting for arena space");
     q.id = s->next_id++;
     q.tree = tree_id;
     q.nq = nq;
@@ -863,7 +900,7 @@ int crt_server_release(crt_server h, int64_t request_id)
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->finished.find(request_id);
   if (it == s->finished.end()) return fail(CRT_ERR_INVALID_ARG, "server_release: unknown request");
-  s->alloc.release(it->second.win_off, it->second.win_bytes);
+  if (it->second.win_bytes) s->alloc.release(it->second.win_off, it->second.win_bytes);
   if (it->second.out_bytes) s->alloc.release(it->second.out_off, it->second.out_bytes);
   s->finished.erase(it);
   return CRT_OK;

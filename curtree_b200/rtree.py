@@ -221,6 +221,38 @@ def canonicalize(fid, tid, stream=None) -> None:
                                         _stream_handle(stream)), "canonicalize")
 
 
+class PairDigest:
+    """Per-window pair counts and order-independent digests accumulated on
+    the device (crt_pairs_digest): int64 counts and uint64 digests (held in
+    an int64 tensor) for nq windows, plus a count of pairs whose window index
+    fell outside [0, nq)."""
+
+    def __init__(self, nq: int):
+        self.nq = int(nq)
+        self.counts = torch.zeros(max(self.nq, 1), dtype=torch.int64, device="cuda")
+        self.hashes = torch.zeros(max(self.nq, 1), dtype=torch.int64, device="cuda")
+        self.bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def add_ptr(self, fid_ptr: int, tid_ptr: int, n: int, window_base: int = 0, stream=None):
+        if n <= 0:
+            return
+        check(load().crt_pairs_digest(fid_ptr, tid_ptr, int(n), int(window_base), self.nq,
+                                      self.counts.data_ptr(), self.hashes.data_ptr(),
+                                      self.bad.data_ptr(), _stream_handle(stream)),
+              "pairs_digest")
+
+    def add(self, fid, tid, window_base: int = 0, n: int | None = None, stream=None):
+        n = int(fid.numel()) if n is None else int(n)
+        if n:
+            self.add_ptr(fid.data_ptr(), tid.data_ptr(), n, window_base, stream)
+
+    def to_host(self) -> tuple[np.ndarray, np.ndarray, int]:
+        """(counts int64, digests uint64, pairs outside the window range)."""
+        c = self.counts.cpu().numpy()[:self.nq]
+        h = self.hashes.cpu().numpy().view(np.uint64)[:self.nq]
+        return c, h, int(self.bad.item())
+
+
 def query_capacity(pairs: int, mode: int = _lib.CRT_QUERY_PERSISTENT) -> int:
     o = _lib.default_opts(mode=mode)
     return int(load().crt_query_capacity(pairs, ctypes.byref(o)))

@@ -189,6 +189,21 @@ int crt_query_into_f32(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
  * Synchronous; at most INT32_MAX pairs per call. */
 int crt_pairs_canonicalize(int32_t* d_fid, int32_t* d_tid, int64_t n, crt_stream_t stream);
 
+/* Per-window pair counts and order-independent digests of a pair list, for
+ * checking a result of billions of pairs without sorting it.  The reference's
+ * drivers verify a query by sorting the pairs and comparing vectors
+ * (src/rtree_test_frontier.cu:102-123); this is that check in a form whose
+ * value does not depend on pair order.  For each pair i with window
+ * w = d_tid[i] + window_base in [0, nq): d_counts[w] += 1 and
+ * d_hashes[w] += mix(((uint64_t)w << 32) | (uint32_t)d_fid[i]) mod 2^64, where
+ * mix is the splitmix64 finaliser.  Pairs whose window falls outside [0, nq)
+ * are skipped and counted in *d_bad (device int64; may be NULL).  The arrays
+ * accumulate (zero them first), so a result streamed in batches is digested
+ * batch by batch with each batch's window_base.  Asynchronous on `stream`. */
+int crt_pairs_digest(const int32_t* d_fid, const int32_t* d_tid, int64_t n, int64_t window_base,
+                     int64_t nq, int64_t* d_counts, uint64_t* d_hashes, int64_t* d_bad,
+                     crt_stream_t stream);
+
 /* Output slots to allocate for `pairs` hit pairs so that a PERSISTENT query
  * cannot overflow (adds the per-warp reservation slack). */
 int64_t crt_query_capacity(int64_t pairs, const crt_query_opts* opts);

@@ -351,16 +351,17 @@ static void* tree_query_worker(void* p)
 }
 
 /* Per-query hit counts, pair digests and work counters for a window batch
- * against a built tree, over `nthreads` host threads. */
-int orc_tree_query_stats(const float* nxmin, const float* nymin, const float* nxmax,
-                         const float* nymax, const int32_t* npos, const int32_t* nlen,
-                         int64_t rsz, int fanout,
-                         const float* bxmin, const float* bymin, const float* bxmax,
-                         const float* bymax, const int32_t* bid, int64_t nbox,
-                         const float* qxmin, const float* qymin, const float* qxmax,
-                         const float* qymax, int64_t nq,
-                         int64_t* counts, uint64_t* hashes, int64_t* tested,
-                         int64_t* nodes_visited, int nthreads)
+ * against a built tree, over `nthreads` host threads.  qid (may be NULL:
+ * positional) gives each query's window index for the digests. */
+int orc_tree_query_stats_ids(const float* nxmin, const float* nymin, const float* nxmax,
+                             const float* nymax, const int32_t* npos, const int32_t* nlen,
+                             int64_t rsz, int fanout,
+                             const float* bxmin, const float* bymin, const float* bxmax,
+                             const float* bymax, const int32_t* bid, int64_t nbox,
+                             const float* qxmin, const float* qymin, const float* qxmax,
+                             const float* qymax, const int32_t* qid, int64_t nq,
+                             int64_t* counts, uint64_t* hashes, int64_t* tested,
+                             int64_t* nodes_visited, int nthreads)
 {
   if (nthreads < 1) nthreads = 1;
   if (nthreads > 256) nthreads = 256;
@@ -375,7 +376,7 @@ int orc_tree_query_stats(const float* nxmin, const float* nymin, const float* nx
     a->npos = npos; a->nlen = nlen; a->rsz = rsz; a->fanout = fanout;
     a->bxmin = bxmin; a->bymin = bymin; a->bxmax = bxmax; a->bymax = bymax; a->bid = bid;
     a->nbox = nbox;
-    a->qxmin = qxmin; a->qymin = qymin; a->qxmax = qxmax; a->qymax = qymax;
+    a->qxmin = qxmin; a->qymin = qymin; a->qxmax = qxmax; a->qymax = qymax; a->qid = qid;
     a->q0 = t * per; a->q1 = (t + 1) * per < nq ? (t + 1) * per : nq;
     a->counts = counts; a->hashes = hashes; a->tested = tested; a->nodes_visited = nodes_visited;
     started[t] = 0;
@@ -389,6 +390,22 @@ int orc_tree_query_stats(const float* nxmin, const float* nymin, const float* nx
     if (args[t].status != 0) st = args[t].status;
   }
   return st;
+}
+
+/* orc_tree_query_stats_ids with positional window indices. */
+int orc_tree_query_stats(const float* nxmin, const float* nymin, const float* nxmax,
+                         const float* nymax, const int32_t* npos, const int32_t* nlen,
+                         int64_t rsz, int fanout,
+                         const float* bxmin, const float* bymin, const float* bxmax,
+                         const float* bymax, const int32_t* bid, int64_t nbox,
+                         const float* qxmin, const float* qymin, const float* qxmax,
+                         const float* qymax, int64_t nq,
+                         int64_t* counts, uint64_t* hashes, int64_t* tested,
+                         int64_t* nodes_visited, int nthreads)
+{
+  return orc_tree_query_stats_ids(nxmin, nymin, nxmax, nymax, npos, nlen, rsz, fanout, bxmin,
+                                  bymin, bxmax, bymax, bid, nbox, qxmin, qymin, qxmax, qymax,
+                                  NULL, nq, counts, hashes, tested, nodes_visited, nthreads);
 }
 
 /* Tree query writing every hit pair (fid = box id, tid = query index) in

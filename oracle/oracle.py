@@ -60,6 +60,9 @@ def lib():
             [_f32p] * 4 + [_i64]
         L.orc_tree_query_stats.restype = ctypes.c_int
         L.orc_tree_query_stats.argtypes = tree_args + [_i64p, _u64p, _i64p, _i64p, ctypes.c_int]
+        L.orc_tree_query_stats_ids.restype = ctypes.c_int
+        L.orc_tree_query_stats_ids.argtypes = tree_args[:-1] + [_i32p, _i64] + \
+            [_i64p, _u64p, _i64p, _i64p, ctypes.c_int]
         L.orc_tree_query_pairs.restype = _i64
         L.orc_tree_query_pairs.argtypes = tree_args + [_i32p, _i32p, _i64]
         nl_args = [_f32p] * 4 + [_i32p, _i64] + [_f32p] * 4 + [_i32p, _i64]
@@ -88,6 +91,9 @@ def ref_cpu():
         R.ref_nested_loop_query.argtypes = args + [_i32p, _i32p, _i64]
         R.ref_nested_loop_query_mt.restype = _i64
         R.ref_nested_loop_query_mt.argtypes = args + [ctypes.c_int]
+        R.ref_nested_loop_query_mt_digest.restype = _i64
+        R.ref_nested_loop_query_mt_digest.argtypes = args + [ctypes.c_int, _i64p, _u64p,
+                                                             ctypes.POINTER(ctypes.c_double)]
         R.ref_read_mbr.restype = ctypes.c_int
         R.ref_read_mbr.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_float] + [_f32p] * 4 + [_i32p]
         _ref = R
@@ -195,15 +201,23 @@ class QueryStats:
         return int(self.counts.sum())
 
 
-def tree_query_stats(tree: HostTree, sboxes, q, nthreads: int | None = None) -> QueryStats:
+def tree_query_stats(tree: HostTree, sboxes, q, nthreads: int | None = None,
+                     qid: np.ndarray | None = None) -> QueryStats:
     """Per-query counts/digests of the reference's tree query semantics
-    (src/rtree_bfs_frontier.cuh:60-289, src/rtree_bfs_thrust.cuh:95-250)."""
+    (src/rtree_bfs_frontier.cuh:60-289, src/rtree_bfs_thrust.cuh:95-250).
+    qid: the windows' indices used in the digests (default: positional)."""
     nthreads = nthreads or os.cpu_count() or 1
     nq = max(q.n, 1)
     st = QueryStats(np.zeros(nq, np.int64), np.zeros(nq, np.uint64), np.zeros(nq, np.int64),
                     np.zeros(nq, np.int64))
-    rc = lib().orc_tree_query_stats(*_tree_args(tree, sboxes, q), st.counts, st.hashes, st.tested,
-                                    st.visited, nthreads)
+    if qid is None:
+        rc = lib().orc_tree_query_stats(*_tree_args(tree, sboxes, q), st.counts, st.hashes,
+                                        st.tested, st.visited, nthreads)
+    else:
+        a = _tree_args(tree, sboxes, q)
+        ids = _c(qid, np.int32) if q.n else np.zeros(1, np.int32)
+        rc = lib().orc_tree_query_stats_ids(*a[:-1], ids, a[-1], st.counts, st.hashes, st.tested,
+                                            st.visited, nthreads)
     if rc != 0:
         raise RuntimeError(f"oracle tree query failed ({rc})")
     if q.n == 0:
@@ -257,6 +271,21 @@ def ref_nested_loop_pairs(q, d, positional_qid: bool = True) -> tuple[np.ndarray
     qo = np.empty(max(n, 1), np.int32)
     R.ref_nested_loop_query(*args, did, qo, n)
     return did[:n], qo[:n]
+
+
+def ref_nested_loop_digest(q, d, qid, nthreads: int | None = None):
+    """The reference's own nested_loop_query over window slices on host
+    threads, with each window's pair count and digest taken from the pairs
+    it emitted (qid = the windows' indices, used as the digest's window).
+    Returns (counts, hashes, pairs, seconds of the nested_loop_query calls)."""
+    nthreads = nthreads or os.cpu_count() or 1
+    counts = np.zeros(max(q.n, 1), np.int64)
+    hashes = np.zeros(max(q.n, 1), np.uint64)
+    secs = ctypes.c_double(0)
+    n = ref_cpu().ref_nested_loop_query_mt_digest(*_box_args(q), _c(qid, np.int32), q.n,
+                                                  *_box_args(d), _c(d.id, np.int32), d.n,
+                                                  nthreads, counts, hashes, ctypes.byref(secs))
+    return counts[:q.n], hashes[:q.n], int(n), secs.value
 
 
 def ref_read_mbr(path: str, n: int, r: float):

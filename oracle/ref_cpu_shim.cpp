@@ -3,7 +3,9 @@
 // sources where they lie into oracle/_ref/libref_cpu.so by oracle/Makefile.
 // TEST INFRASTRUCTURE ONLY: used to pin the oracle and as the timed CPU
 // baseline of the benchmark; never linked into the product library.
+#include <algorithm>
 #include <cassert>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <iostream>
@@ -83,6 +85,73 @@ extern "C" int64_t ref_nested_loop_query_mt(const float* qxmin, const float* qym
   int64_t total = 0;
   for (auto c : counts) total += c;
   return total;
+}
+
+namespace {
+// splitmix64 finaliser: the per-pair digest of the oracle (orc_pair_hash).
+inline uint64_t mix64(uint64_t z)
+{
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+// ref_nested_loop_query_mt, keeping each slice's output: after the
+// reference's nested_loop_query calls (timed alone, wall clock of the
+// parallel section, into *query_seconds), each thread reduces its pairs to
+// per-query counts and order-independent digests, counts[i] / hashes[i] for
+// query i, digest = sum of mix64((uint64)(uint32)qid << 32 | (uint32)did)
+// over the pairs the reference emitted for it (qid[i] is its window index).
+// Returns the total pair count.
+extern "C" int64_t ref_nested_loop_query_mt_digest(const float* qxmin, const float* qymin,
+                                                   const float* qxmax, const float* qymax,
+                                                   const int* qid, int nq, const float* dxmin,
+                                                   const float* dymin, const float* dxmax,
+                                                   const float* dymax, const int* did, int nd,
+                                                   int nthreads, int64_t* counts,
+                                                   uint64_t* hashes, double* query_seconds)
+{
+  if (nthreads < 1) nthreads = 1;
+  std::vector<int64_t> total(nthreads, 0);
+  std::vector<std::chrono::steady_clock::time_point> ends(nthreads);
+  std::vector<std::thread> th;
+  int per = (nq + nthreads - 1) / nthreads;
+  const auto start = std::chrono::steady_clock::now();
+  for (int t = 0; t < nthreads; t++) {
+    int q0 = t * per, q1 = std::min(nq, (t + 1) * per);
+    if (q0 >= q1) {
+      ends[t] = start;
+      continue;
+    }
+    th.emplace_back([=, &total, &ends] {
+      BBOX<float> q = make_box(qxmin + q0, qymin + q0, qxmax + q0, qymax + q0, qid + q0, q1 - q0);
+      BBOX<float> d = make_box(dxmin, dymin, dxmax, dymax, did, nd);
+      thrust::host_vector<int> v_did, v_qid;
+      total[t] = nested_loop_query<float>(q, d, v_did, v_qid);
+      ends[t] = std::chrono::steady_clock::now();
+      for (int i = q0; i < q1; i++) {
+        counts[i] = 0;
+        hashes[i] = 0;
+      }
+      // the reference emits queries in order, each query's pairs together
+      int i = q0;
+      for (size_t k = 0; k < v_did.size(); k++) {
+        while (i < q1 && v_qid[k] != qid[i]) i++;
+        if (i >= q1) break;
+        counts[i]++;
+        hashes[i] += mix64(((uint64_t)(uint32_t)v_qid[k] << 32) | (uint32_t)v_did[k]);
+      }
+    });
+  }
+  for (auto& t : th) t.join();
+  auto end = start;
+  for (auto e : ends) end = std::max(end, e);
+  if (query_seconds) *query_seconds = std::chrono::duration<double>(end - start).count();
+  int64_t sum = 0;
+  for (auto c : total) sum += c;
+  return sum;
 }
 
 // The reference's readMBR (src/utility.cpp:5-40), compiled from its source,

@@ -344,3 +344,63 @@ def test_plain_csr_without_window_column(crt):
         crt.query_into(rt, d, dq, fid2, None, res, None, crt.CRT_QUERY_PLAIN)
     with pytest.raises(crt.CrtError):
         crt.query_into(rt, d, dq, fid2, None, res, offs2, crt.CRT_QUERY_PERSISTENT)
+
+
+def test_pairs_digest_matches_oracle(crt):
+    """crt_pairs_digest gives the oracle's per-window counts and digests:
+    random pairs, a window base offset, pairs outside the window range
+    (skipped and counted), and long runs of one window across whole warps
+    (the warp-aggregated path), in pieces accumulated call by call."""
+    import torch
+    rng = np.random.default_rng(11)
+    nq = 5000
+    parts = []
+    # scattered windows, random ids (negative ones included)
+    parts.append((rng.integers(-2**31, 2**31, 200_003).astype(np.int32),
+                  rng.integers(0, nq, 200_003).astype(np.int32)))
+    # long runs: a few windows with 100k+ consecutive pairs each
+    runs = np.repeat(np.array([7, 4999, 0, 1234], np.int32), [130_000, 70_001, 4096, 99_999])
+    parts.append((rng.integers(-2**31, 2**31, runs.size).astype(np.int32), runs))
+    dg = crt.PairDigest(nq)
+    want_c = np.zeros(nq, np.int64)
+    want_h = np.zeros(nq, np.uint64)
+    for fid, tid in parts:
+        dg.add(torch.from_numpy(fid).cuda(), torch.from_numpy(tid).cuda())
+        c, h = O.pair_hashes(fid, tid, nq)
+        want_c += c
+        with np.errstate(over="ignore"):
+            want_h += h
+    # a batch whose window indices are relative to a base; some fall outside
+    base = 3000
+    fid = rng.integers(-2**31, 2**31, 50_000).astype(np.int32)
+    tid = rng.integers(-100, nq - base + 100, 50_000).astype(np.int32)
+    dg.add(torch.from_numpy(fid).cuda(), torch.from_numpy(tid).cuda(), window_base=base)
+    w = tid.astype(np.int64) + base
+    ok = (w >= 0) & (w < nq)
+    c, h = O.pair_hashes(fid[ok], w[ok].astype(np.int32), nq)
+    want_c += c
+    with np.errstate(over="ignore"):
+        want_h += h
+    gc, gh, bad = dg.to_host()
+    assert bad == int((~ok).sum()) and bad > 0
+    assert np.array_equal(gc, want_c)
+    assert np.array_equal(gh, want_h)
+
+
+def test_pairs_digest_of_a_query_equals_oracle_stats(crt):
+    """The digest of a persistent query's output equals the oracle's tree
+    query counts and digests for every window."""
+    b = D.clustered_boxes(300_000, seed=17)
+    q = D.mixed_windows(20_000, b, seed=117)
+    d = crt.BBox.from_host(b)
+    rt = crt.RTree(16)
+    crt.build_rtree(d, rt)
+    dq = crt.BBox.from_host(q)
+    fid, tid = crt.query(rt, d, dq)
+    dg = crt.PairDigest(q.n)
+    dg.add(fid, tid)
+    sb, t = O.build(b, 16)
+    want = O.tree_query_stats(t, sb, q)
+    gc, gh, bad = dg.to_host()
+    assert bad == 0 and want.total > 100_000
+    assert np.array_equal(gc, want.counts) and np.array_equal(gh, want.hashes)

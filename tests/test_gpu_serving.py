@@ -157,3 +157,68 @@ def test_device_wait_timeout_is_reported(env):
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
     srv.release(rid)
     srv.close()
+
+
+def _wait_for(srv, rid, timeout_s=30.0):
+    t0 = time.monotonic()
+    while time.monotonic() - t0 < timeout_s:
+        for c in srv.poll(max_out=16, wait_ms=10):
+            if c["request_id"] == rid:
+                return c
+            srv.release(c["request_id"])
+    raise AssertionError(f"request {rid} did not complete within {timeout_s} s")
+
+
+def test_rerun_after_fragmentation(env):
+    """A re-run whose exact output fits the arena only as one block with its
+    windows: the request's window block sits in the middle of the arena
+    (after a large request that completed and was released), so neither hole
+    beside it can hold the output.  The re-run moves its windows out and back
+    and completes with the oracle's pairs; a re-run that can never fit ends
+    with CRT_ERR_OOM.  Both within 30 s, with the device loop idle between."""
+    C, Server, trees = env
+    t = trees[0]
+    arena = 32 << 20
+    srv, ids = setup_server(C, Server, trees, arena_bytes=arena, pairs_per_window=0.001,
+                            output_slack=0.01)
+    # R0: 1M windows far outside the tree (no hits): a 16 MB window block at
+    # the start of the arena
+    n0 = 1_000_000
+    far = np.full(n0, -2.0e6, np.float32)
+    r0 = D.HostBoxes(far, far, far + 1, far + 1, np.arange(n0, dtype=np.int32))
+    # R1: windows whose exact output (2.6M-3.6M pairs) is larger than either
+    # hole left around R1's windows once R0 is released
+    pool = D.uniform_windows(20_000, seed=79, max_side=0.09)
+    counts = C.query_stats(t["rt"], t["d"], C.BBox.from_host(pool),
+                           per_window=True)["per_window_hits"].cpu().numpy()
+    cum = np.cumsum(counts)
+    k = int(np.searchsorted(cum, 3_000_000)) + 1
+    assert 2_600_000 <= cum[k - 1] <= 3_600_000
+    r1 = pool.take(np.arange(k))
+    need = int(cum[k - 1])
+    assert need * 8 > arena // 2 and need * 8 + 16 * k + 512 < arena
+    a = srv.submit(ids[0], r0)
+    b = srv.submit(ids[0], r1)
+    assert a is not None and b is not None
+    t0 = time.monotonic()
+    ca = _wait_for(srv, a)
+    assert ca["status"] == 0 and ca["count"] == 0
+    srv.release(a)
+    cb = _wait_for(srv, b)
+    assert cb["status"] == 0 and cb["retries"] >= 1 and cb["count"] == need
+    got = O.canonical_pairs(*Server.pairs(cb))
+    want = expected(trees, 0, r1)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    srv.release(b)
+    # a re-run whose exact output is larger than the whole arena fails cleanly
+    k2 = int(np.searchsorted(cum, 6_000_000)) + 1
+    r2 = pool.take(np.arange(k2))
+    c = srv.submit(ids[0], r2)
+    assert c is not None
+    cc = _wait_for(srv, c)
+    assert cc["status"] == C._lib.CRT_ERR_OOM and cc["count"] == int(cum[k2 - 1])
+    srv.release(c)
+    assert time.monotonic() - t0 < 30
+    st = srv.stats()
+    assert st["arena_used"] == 0 and st["retried"] >= 2
+    assert srv.close() == 0

@@ -66,3 +66,49 @@ def test_noalloc_plain_query_matches_allocating_plain_query():
                                        None, None, 0, res.data_ptr(), _stream_handle(None))
     assert st == _lib.CRT_ERR_INVALID_ARG
     assert b"65536" in L.crt_last_error()
+
+
+def test_noalloc_plain_query_matches_oracle_and_reports_overflow():
+    """The allocation-free plain query against the oracle's pairs (bit-exact
+    canonical sets) at the 65536-window limit, and with an output one pair too
+    small: the result block reports overflow and the exact pair count, and a
+    retry at that size succeeds -- on the same shared scratch."""
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import curtree_b200 as C
+    from curtree_b200 import _lib
+    from curtree_b200.rtree import _stream_handle
+    from oracle import oracle as O
+
+    L = _lib.load()
+    b = D.clustered_boxes(200_000, seed=92)
+    d = C.BBox.from_host(b)
+    rt = C.RTree(16)
+    C.build_rtree(d, rt)
+    q = D.mixed_windows(65_536, b, seed=192, lo=1e-5, hi=2e-2)
+    dq = C.BBox.from_host(q)
+    sb, t = O.build(b, 16)
+    want = O.canonical_pairs(*O.tree_query_pairs(t, sb, q))
+    n = len(want[0])
+    assert n > 50_000
+
+    rb, qb = d.c(), dq.c()
+
+    def call(cap):
+        fid = torch.full((max(cap, 1),), -1, dtype=torch.int32, device="cuda")
+        tid = torch.full((max(cap, 1),), -1, dtype=torch.int32, device="cuda")
+        res = C.new_result_block()
+        st = L.crt_query_plain_noalloc_f32(ctypes.byref(rt.s), ctypes.byref(rb), ctypes.byref(qb),
+                                           fid.data_ptr(), tid.data_ptr(), cap, res.data_ptr(),
+                                           _stream_handle(None))
+        assert st == _lib.CRT_OK, L.crt_last_error()
+        return fid, tid, C.read_result(res)
+
+    fid, tid, r = call(n - 1)
+    assert r["overflow"] == 1 and r["required"] == n and r["count"] == 0 and r["error"] == 0, r
+    fid, tid, r = call(n)
+    assert r["overflow"] == 0 and r["count"] == n and r["error"] == 0, r
+    got = O.canonical_pairs(fid.cpu().numpy(), tid.cpu().numpy())
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    # grouped by window, in window order
+    assert np.all(np.diff(tid.cpu().numpy()) >= 0)
