@@ -34,11 +34,9 @@ struct alignas(32) Box32 {
   int4 idp;    // id, 0, 0, 0
 };
 
-constexpr int kRadixBits = 8;
 constexpr int kSortThreads = 512;
 constexpr int kSortIpt = kSortTile / kSortThreads;  // 16 keys per thread
 constexpr int kSortWarps = kSortThreads / 32;
-static_assert(kBins == 1 << kRadixBits, "digit width");
 using BuildCtrl = SortCtrl;
 
 constexpr uint64_t kFlagAgg = 1ull << 62;
@@ -60,6 +58,9 @@ constexpr uint64_t kFlagIncl = 2ull << 62;
 constexpr int kEncThreads = 256;
 constexpr int kEncGroups = 4;                            // float4 groups per thread
 constexpr int kEncTile = 4 * kEncGroups * kEncThreads;   // 4096 boxes
+constexpr int kGroups = 256;                             // record runs: by the key's top byte
+static_assert(kDigits * kDigitBits - kDigitBits >= 24, "the last digit lies in the top byte");
+static_assert(kGroups <= kEncThreads, "one thread per run");
 
 struct BoxIn {
   const float* __restrict__ xmin;
@@ -105,17 +106,17 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
                                                              Box32* __restrict__ aos,
                                                              uint32_t* __restrict__ hist)
 {
-  __shared__ uint32_t sh[3][kBins];  // digits 0..2 over all of this CTA's tiles
-  __shared__ uint32_t s_top[kBins];  // digit 3 over all of this CTA's tiles
-  __shared__ uint32_t s_run[kBins];  // this tile: count, then run start, per top digit
-  __shared__ uint32_t s_wsum[kBins / 32];
-  __shared__ uint32_t s_dr[kEncTile];  // per box of the tile: top digit << 16 | rank in its run
+  // digit histograms over all of this CTA's tiles (the last digit lies in
+  // the top byte: it is added from the tile's top-byte counts)
+  __shared__ uint32_t sh[kDigits][kBins];
+  __shared__ uint32_t s_run[kGroups];  // this tile: count, then run start, per top byte
+  __shared__ uint32_t s_wsum[kGroups / 32];
+  __shared__ uint32_t s_dr[kEncTile];  // per box of the tile: top byte << 16 | rank in its run
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < 3 * kBins; i += kEncThreads) (&sh[0][0])[i] = 0;
-  if (tid < kBins) s_top[tid] = 0;
+  for (int i = tid; i < kDigits * kBins; i += kEncThreads) (&sh[0][0])[i] = 0;
   const int64_t ntiles = (n + kEncTile - 1) / kEncTile;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    if (tid < kBins) s_run[tid] = 0;
+    if (tid < kGroups) s_run[tid] = 0;
     __syncthreads();
     const int64_t base = t * kEncTile;
 #pragma unroll
@@ -136,9 +137,8 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
         if (j + k < n) {
           const uint32_t top = kk[k] >> 24;
           s_dr[i0 + k] = top << 16 | atomicAdd(&s_run[top], 1u);
-          atomicAdd(&sh[0][kk[k] & 0xFF], 1u);
-          atomicAdd(&sh[1][(kk[k] >> 8) & 0xFF], 1u);
-          atomicAdd(&sh[2][(kk[k] >> 16) & 0xFF], 1u);
+#pragma unroll
+          for (int dg = 0; dg < kDigits - 1; dg++) atomicAdd(&sh[dg][key_digit(kk[k], dg)], 1u);
         }
       }
       if (j + 3 < n) {
@@ -149,11 +149,11 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
       }
     }
     __syncthreads();
-    // run starts: exclusive prefix of the tile's top-digit counts
+    // run starts: exclusive prefix of the tile's top-byte counts
     uint32_t cnt = 0, x = 0;
-    if (tid < kBins) {
+    if (tid < kGroups) {
       cnt = s_run[tid];
-      s_top[tid] += cnt;
+      if (cnt) atomicAdd(&sh[kDigits - 1][key_digit((uint32_t)tid << 24, kDigits - 1)], cnt);
       x = cnt;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
       if (lane == 31) s_wsum[warp] = x;
     }
     __syncthreads();
-    if (tid < kBins) {
+    if (tid < kGroups) {
       uint32_t start = x - cnt;
       for (int w = 0; w < warp; w++) start += s_wsum[w];
       s_run[tid] = start;
@@ -203,42 +203,46 @@ __global__ void __launch_bounds__(kEncThreads) encode_kernel(BoxIn in, int64_t n
     }
     __syncthreads();
   }
-  for (int i = tid; i < 3 * kBins; i += kEncThreads) {
+  for (int i = tid; i < kDigits * kBins; i += kEncThreads) {
     const uint32_t v = (&sh[0][0])[i];
     if (v) atomicAdd(&hist[i], v);
   }
-  if (tid < kBins && s_top[tid]) atomicAdd(&hist[3 * kBins + tid], s_top[tid]);
 }
 
 // ---------------------------------------------------------------------------
 // 2. plan
 // ---------------------------------------------------------------------------
+// One warp per digit: a digit whose histogram has one bin holding every key
+// is uniform and its pass is skipped (a stable pass over a uniform digit
+// leaves the order unchanged); the exclusive prefix of the bins is each
+// bucket's global start.
 __global__ void plan_kernel(const uint32_t* __restrict__ hist, int64_t n, BuildCtrl* ctrl)
 {
-  __shared__ int s_uniform[4];
-  if (threadIdx.x < 4) s_uniform[threadIdx.x] = 0;
+  __shared__ int s_uniform[kDigits];
+  if (threadIdx.x < kDigits) s_uniform[threadIdx.x] = 0;
   __syncthreads();
-  // one warp per digit: exclusive scan of its 256 bins
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (w < 4) {
+  if (w < kDigits) {
+    const int nb = 1 << digit_bits(w);
     uint32_t carry = 0;
-    for (int c = 0; c < kBins; c += 32) {
-      uint32_t v = hist[w * kBins + c + l];
-      if ((int64_t)v == n) s_uniform[w] = 1;
+    for (int c = 0; c < nb; c += 32) {
+      const bool in = c + l < nb;
+      const uint32_t v = in ? hist[w * kBins + c + l] : 0u;
+      if (in && (int64_t)v == n) s_uniform[w] = 1;
       uint32_t x = v;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (l >= o) x += y;
       }
-      ctrl->bucket_start[w * kBins + c + l] = (int)(carry + x - v);
+      if (in) ctrl->bucket_start[w * kBins + c + l] = (int)(carry + x - v);
       carry += __shfl_sync(0xffffffffu, x, 31);
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     int act = 0, na = 0;
-    for (int d = 0; d < 4; d++)
+    for (int d = 0; d < kDigits; d++)
       if (!s_uniform[d]) { act |= 1 << d; na++; }
     ctrl->active = act;
     ctrl->n_active = na;
@@ -248,14 +252,10 @@ __global__ void plan_kernel(const uint32_t* __restrict__ hist, int64_t n, BuildC
 // ---------------------------------------------------------------------------
 // 3. onesweep pass
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t digit_of(uint32_t k, int shift)
-{
-  return (k >> shift) & 0xFFu;
-}
-
 // Lanes of the warp whose value equals this lane's (v < 2^kBits), from one
 // ballot per bit; on this part it issues faster than __match_any_sync
-// (measured over the four passes of a 100M-key build: 3.7 ms against 4.3 ms).
+// (measured over the four 8-bit passes of a 100M-key build: 3.7 ms against
+// 4.3 ms).
 template <int kBits>
 __device__ __forceinline__ uint32_t peer_mask(uint32_t v)
 {
@@ -274,25 +274,41 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Shared memory of one pass: (key, slot) pairs staged in destination order,
-// the tile's incoming slots (prefetched while the tile is ranked), and the
-// per-warp digit counters (16-bit: at most 8192 per tile).
-constexpr size_t kSortSmem = (size_t)kSortTile * 8 + (size_t)kSortTile * 4 +
-                             (size_t)kSortWarps * kBins * 2;
+// Shared memory of one pass over a kBits-bit digit: keys and values staged in
+// destination order, the tile's incoming values prefetched while the tile is
+// ranked (narrow digits only: with 1024 bins the per-warp counters take that
+// room, and the values are copied straight to their staged slots instead),
+// the per-warp digit counters (16-bit: at most 8192 per tile), the bins'
+// global offsets and the warp sums of the bin scan.
+template <int kBits>
+struct SweepSmem {
+  static constexpr int kB = 1 << kBits;
+  static constexpr bool kPrefetch = kBits <= 8;
+  static constexpr size_t kKeys = 0;
+  static constexpr size_t kVals = kKeys + 4 * (size_t)kSortTile;
+  static constexpr size_t kVin = kVals + 4 * (size_t)kSortTile;
+  static constexpr size_t kHist = kVin + (kPrefetch ? 4 * (size_t)kSortTile : 0);
+  static constexpr size_t kGbase = kHist + 2 * (size_t)kSortWarps * (kB < 2 ? 2 : kB);
+  static constexpr size_t kWsum = kGbase + 4 * (size_t)kB;
+  static constexpr size_t kBytes = kWsum + 4 * 32;
+};
+static_assert(2 * (SweepSmem<10>::kBytes + 1024) <= 227 * 1024, "two 10-bit CTAs per SM");
+static_assert(2 * (SweepSmem<8>::kBytes + 1024) <= 227 * 1024, "two 8-bit CTAs per SM");
 
 // Ranks this thread's keys inside its warp, stably (rounds in order, lanes in
 // order).  kFull: every item of the tile is valid (no bounds checks, and the
-// digit fits 8 bits, so 8 ballots); otherwise invalid items take digit 256.
-template <bool kFull>
+// digit fits kBits bits); otherwise invalid items take digit 2^kBits.
+template <bool kFull, int kBits>
 __device__ __forceinline__ void rank_keys(const uint32_t (&key)[kSortIpt], uint32_t (&rank)[kSortIpt],
                                           uint16_t* wh, int wbase, int tile_n, int shift)
 {
+  constexpr uint32_t kMask = (1u << kBits) - 1u;
   const uint32_t lt = lanemask_lt();
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
     const bool v = kFull || wbase + 32 * i < tile_n;
-    const uint32_t dig = v ? digit_of(key[i], shift) : kBins;
-    const uint32_t peers = kFull ? peer_mask<8>(dig) : peer_mask<9>(dig);
+    const uint32_t dig = v ? (key[i] >> shift) & kMask : kMask + 1u;
+    const uint32_t peers = kFull ? peer_mask<kBits>(dig) : peer_mask<kBits + 1>(dig);
     const uint32_t old = v ? wh[dig] : 0u;
     __syncwarp();
     if (v && (peers & lt) == 0) wh[dig] = (uint16_t)(old + __popc(peers));
@@ -301,19 +317,27 @@ __device__ __forceinline__ void rank_keys(const uint32_t (&key)[kSortIpt], uint3
   }
 }
 
-// One stable LSD pass over (key, slot) pairs for the 8-bit digit at `digit`.
-// Indices are 32-bit: the key count is below 2^31 (the C ABI's int sizes).
+// One stable LSD pass over (key, value) pairs for the kBits-bit digit at
+// `digit` (bits digit * kDigitBits ...), with decoupled look-back across
+// tiles.  Indices are 32-bit: the key count is below 2^31 (the C ABI's int
+// sizes).
+template <int kBits>
 __global__ void __launch_bounds__(kSortThreads, 2)
     onesweep_kernel(int digit, SortBufs bufs, int64_t n64, uint64_t* __restrict__ status,
                     BuildCtrl* __restrict__ ctrl, int flags)
 {
-  extern __shared__ __align__(16) unsigned char smem[];
-  uint2* s_kv = (uint2*)smem;                                       // kSortTile
-  uint32_t* s_vin = (uint32_t*)(smem + (size_t)kSortTile * 8);      // kSortTile
-  uint16_t* s_whist = (uint16_t*)(smem + (size_t)kSortTile * 12);   // kSortWarps x kBins
-  __shared__ int s_gbase[kBins];
+  using L = SweepSmem<kBits>;
+  constexpr int kB = L::kB;
+  constexpr uint32_t kMask = (uint32_t)kB - 1u;
+  constexpr int kBPT = (kB + kSortThreads - 1) / kSortThreads;  // bins per thread
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  uint32_t* s_key = (uint32_t*)(sweep_smem + L::kKeys);
+  uint32_t* s_val = (uint32_t*)(sweep_smem + L::kVals);
+  uint32_t* s_vin = (uint32_t*)(sweep_smem + L::kVin);
+  uint16_t* s_whist = (uint16_t*)(sweep_smem + L::kHist);
+  int* s_gbase = (int*)(sweep_smem + L::kGbase);
+  int* s_wsum = (int*)(sweep_smem + L::kWsum);
   __shared__ int s_tile;
-  __shared__ int s_wsum[kBins / 32];
 
   const int active = ctrl->active;
   if (!((active >> digit) & 1)) return;
@@ -321,12 +345,13 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   const int parity = __popc(before) & 1;
   const bool first = before == 0 && !(flags & kSortGivenValues);
   const bool last = (active >> (digit + 1)) == 0 && !(flags & kSortKeepKeys);
-  const int shift = digit * kRadixBits;
+  const int shift = digit * kDigitBits;
   const int n = (int)n64;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(&ctrl->tile_ctr[digit], 1);
-  for (int i = tid; i < kSortWarps * kBins / 2; i += kSortThreads) ((uint32_t*)s_whist)[i] = 0;
+  for (int i = tid; i < kSortWarps * kB / 2; i += kSortThreads) ((uint32_t*)s_whist)[i] = 0;
+  if (kB < 2 && tid < kSortWarps) s_whist[tid] = 0;
   __syncthreads();
   const int tile = s_tile;
   const int base = tile * kSortTile;
@@ -337,9 +362,9 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   uint32_t* __restrict__ dst_v = bufs.vals[parity ^ 1];
   const int wbase = warp * 32 * kSortIpt + lane;  // this lane's first item in the tile
 
-  // the tile's incoming slots land in shared memory while the keys are ranked
-  // (16-byte async copies; the tile start is 32 KiB-aligned)
-  if (!first) {
+  // the tile's incoming values land in shared memory while the keys are
+  // ranked (16-byte async copies; the tile start is 32 KiB-aligned)
+  if (L::kPrefetch && !first) {
 #pragma unroll
     for (int c = tid; c < kSortTile / 4; c += kSortThreads) {
       const int left = tile_n - 4 * c;
@@ -356,97 +381,126 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   // load keys (warp-striped: item i of a lane is wbase + 32 i)
   uint32_t key[kSortIpt];
   uint32_t rank[kSortIpt];
-  uint16_t* wh = s_whist + warp * kBins;
+  uint16_t* wh = s_whist + warp * kB;
   if (tile_n == kSortTile) {
 #pragma unroll
     for (int i = 0; i < kSortIpt; i++) key[i] = src_k[wbase + 32 * i];
-    rank_keys<true>(key, rank, wh, wbase, tile_n, shift);
+    rank_keys<true, kBits>(key, rank, wh, wbase, tile_n, shift);
   } else {
 #pragma unroll
     for (int i = 0; i < kSortIpt; i++) {
       const int j = wbase + 32 * i;
       key[i] = j < tile_n ? src_k[j] : 0u;
     }
-    rank_keys<false>(key, rank, wh, wbase, tile_n, shift);
+    rank_keys<false, kBits>(key, rank, wh, wbase, tile_n, shift);
   }
   __syncthreads();
-  // per bin: exclusive prefix over warps, the tile count, and the tile-local bin start
-  int cnt = 0;
-  if (tid < kBins) {
+  // per owned bin: exclusive prefix over warps and the tile count
+  int cnt[kBPT];
+  int tsum = 0;
+#pragma unroll
+  for (int j = 0; j < kBPT; j++) {
+    const int b = tid * kBPT + j;
     int run = 0;
+    if (b < kB) {
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-      const int c = (int)s_whist[w * kBins + tid];
-      s_whist[w * kBins + tid] = (uint16_t)run;
-      run += c;
-    }
-    cnt = run;
-    int x = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) s_wsum[warp] = x;
-    s_gbase[tid] = x - cnt;  // within this 32-bin group, completed below
-  }
-  __syncthreads();
-  if (tid < kBins) {
-    int binstart = s_gbase[tid];
-    for (int w = 0; w < warp; w++) binstart += s_wsum[w];
-    // fold the bin start into every warp's offset: one lookup per key later
-#pragma unroll
-    for (int w = 0; w < kSortWarps; w++)
-      s_whist[w * kBins + tid] = (uint16_t)(s_whist[w * kBins + tid] + binstart);
-
-    // decoupled look-back for bin `tid`
-    int excl = 0;
-    if (tile == 0) {
-      st_relaxed_u64(&status[tid], kFlagIncl | (uint32_t)cnt);
-    } else {
-      st_relaxed_u64(&status[(int64_t)tile * kBins + tid], kFlagAgg | (uint32_t)cnt);
-      int t = tile - 1;
-      uint32_t spins = 0;
-      while (true) {
-        const uint64_t v = ld_relaxed_u64(&status[(int64_t)t * kBins + tid]);
-        const uint64_t flag = v & (3ull << 62);
-        if (flag == 0) {
-          if (++spins > kSpinLimit || ld_relaxed_i32(&ctrl->error) != 0) {
-            raise_error(&ctrl->error, CRT_ERR_DEVICE_TIMEOUT);
-            break;
-          }
-          if (spins > 64) __nanosleep(64);
-          continue;
-        }
-        excl += (int)(uint32_t)v;
-        if (flag == kFlagIncl) break;
-        --t;
+      for (int w = 0; w < kSortWarps; w++) {
+        const int c = (int)s_whist[w * kB + b];
+        s_whist[w * kB + b] = (uint16_t)run;
+        run += c;
       }
-      st_relaxed_u64(&status[(int64_t)tile * kBins + tid], kFlagIncl | (uint32_t)(excl + cnt));
     }
-    s_gbase[tid] = ctrl->bucket_start[digit * kBins + tid] + excl - binstart;
+    cnt[j] = run;
+    tsum += run;
   }
-  if (!first) asm volatile("cp.async.wait_all;" ::: "memory");
+  // exclusive scan of the per-thread bin sums over the CTA (bins in order)
+  int x = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_wsum[warp] = x;
+  // publish this tile's aggregate of every owned bin before waiting on
+  // predecessors (tile 0 publishes its inclusive count at once)
+#pragma unroll
+  for (int j = 0; j < kBPT; j++) {
+    const int b = tid * kBPT + j;
+    if (b < kB)
+      st_relaxed_u64(&status[(int64_t)tile * kB + b],
+                     (tile == 0 ? kFlagIncl : kFlagAgg) | (uint32_t)cnt[j]);
+  }
+  __syncthreads();
+  int binstart = x - tsum;
+  for (int w = 0; w < warp; w++) binstart += s_wsum[w];
+#pragma unroll
+  for (int j = 0; j < kBPT; j++) {
+    const int b = tid * kBPT + j;
+    if (b < kB) {
+      // fold the bin start into every warp's offset: one lookup per key later
+#pragma unroll
+      for (int w = 0; w < kSortWarps; w++)
+        s_whist[w * kB + b] = (uint16_t)(s_whist[w * kB + b] + binstart);
+      // decoupled look-back for bin b
+      int excl = 0;
+      if (tile > 0) {
+        int t = tile - 1;
+        uint32_t spins = 0;
+        while (true) {
+          const uint64_t v = ld_relaxed_u64(&status[(int64_t)t * kB + b]);
+          const uint64_t flag = v & (3ull << 62);
+          if (flag == 0) {
+            if (++spins > kSpinLimit || ld_relaxed_i32(&ctrl->error) != 0) {
+              raise_error(&ctrl->error, CRT_ERR_DEVICE_TIMEOUT);
+              break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+          }
+          excl += (int)(uint32_t)v;
+          if (flag == kFlagIncl) break;
+          --t;
+        }
+        st_relaxed_u64(&status[(int64_t)tile * kB + b], kFlagIncl | (uint32_t)(excl + cnt[j]));
+      }
+      s_gbase[b] = ctrl->bucket_start[digit * kBins + b] + excl - binstart;
+    }
+    binstart += cnt[j];
+  }
+  if (L::kPrefetch && !first) asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
 
-  // stage (key, slot) pairs in the order of their destination
+  // stage (key, value) pairs in the order of their destination
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
     const int j = wbase + 32 * i;
     if (j < tile_n) {
-      const int pos = (int)(wh[digit_of(key[i], shift)] + rank[i]);
-      s_kv[pos] = make_uint2(key[i], first ? (uint32_t)(base + j) : s_vin[j]);
+      const int pos = (int)(wh[(key[i] >> shift) & kMask] + rank[i]);
+      s_key[pos] = key[i];
+      if (first) {
+        s_val[pos] = (uint32_t)(base + j);
+      } else if (L::kPrefetch) {
+        s_val[pos] = s_vin[j];
+      } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(s_val + pos)),
+                     "l"(src_v + j)
+                     : "memory");
+      }
     }
+  }
+  if (!L::kPrefetch && !first) {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_all;" ::: "memory");
   }
   __syncthreads();
   for (int j = tid; j < tile_n; j += kSortThreads) {
-    const uint2 kv = s_kv[j];
-    const int dst = s_gbase[digit_of(kv.x, shift)] + j;
+    const uint32_t k = s_key[j];
+    const int dst = s_gbase[(k >> shift) & kMask] + j;
     if ((uint32_t)dst < (uint32_t)n) {
       // evict-first: a pass's output is read once, by the next pass, and
       // the look-back status words and the next tiles' runs want L2
-      if (!last) __stcs(dst_k + dst, kv.x);
-      __stcs(dst_v + dst, kv.y);
+      if (!last) __stcs(dst_k + dst, k);
+      __stcs(dst_v + dst, s_val[j]);
     }
   }
 }
@@ -561,6 +615,138 @@ __global__ void __launch_bounds__(kLevelThreads)
 }
 
 // ---------------------------------------------------------------------------
+// 4. leaf level through shared memory
+// ---------------------------------------------------------------------------
+// The leaf-parent level for fanout <= kLeafChunk.  Each CTA takes the
+// parents whose children fill at most kChunk sorted slots:
+//   1. the record slots of those children (coalesced 4-byte loads),
+//   2. two 16-byte async copies per record from the AoS copy into shared
+//      memory (cp.async: the gathers are in flight without holding
+//      registers, so many CTAs per SM keep many gathers in flight),
+//   3. per warp, lanes mapped to (parent, child) as in the traversal: each
+//      lane writes its child's permuted box (nearly contiguous stores) and
+//      the parent's MBR is a segmented min/max over the group's lanes with
+//      shuffles (fminf/fmaxf, reduce_op's device min/max; no neutral
+//      element, so an all-NaN group stays NaN as in the reference).
+constexpr int kLeafThreads = 256;
+constexpr int kLeafWarps = kLeafThreads / 32;
+constexpr int kLeafChunk = 1024;
+
+template <int kChunk>
+__global__ void __launch_bounds__(kLeafThreads, (227 * 1024) / (kChunk * 32 + 1024))
+    leaf_gather_kernel(int fanout, int parents_per_cta, int64_t n, int64_t nparent,
+                       int64_t parent_start, int64_t pos_base, const uint32_t* __restrict__ vals0,
+                       const uint32_t* __restrict__ vals1, const BuildCtrl* __restrict__ ctrl,
+                       const Box32* __restrict__ aos, float* __restrict__ oxmin,
+                       float* __restrict__ oymin, float* __restrict__ oxmax,
+                       float* __restrict__ oymax, int* __restrict__ oid,
+                       float* __restrict__ nxmin, float* __restrict__ nymin,
+                       float* __restrict__ nxmax, float* __restrict__ nymax,
+                       int* __restrict__ npos, int* __restrict__ nlen)
+{
+  extern __shared__ __align__(32) unsigned char leaf_smem[];
+  Box32* s_rec = (Box32*)leaf_smem;
+  const int64_t p0 = (int64_t)blockIdx.x * parents_per_cta;
+  const int64_t p1 = min(nparent, p0 + parents_per_cta);
+  if (p0 >= p1) return;
+  const int f = fanout;
+  const int64_t c0 = p0 * f;
+  const int m = (int)(min(n, p1 * f) - c0);  // <= parents_per_cta * f <= kChunk
+  const uint32_t* __restrict__ sorted = (ctrl->n_active & 1) ? vals1 : vals0;
+
+  constexpr int kPer = kChunk / kLeafThreads;
+  uint32_t src[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int i = threadIdx.x + u * kLeafThreads;
+    uint32_t v = i < m ? __ldg(sorted + c0 + i) : 0u;
+    if ((int64_t)v >= n) v = i < m ? (uint32_t)(c0 + i) : 0u;  // only after a sort error (reported)
+    src[u] = v;
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; u++) {
+    const int i = threadIdx.x + u * kLeafThreads;
+    if (i < m) {
+      const uint32_t d = smem_u32(s_rec + i);
+      const char* g = (const char*)(aos + src[u]);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16u), "l"(g + 16)
+                   : "memory");
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int K, g, c;
+  if (f <= 32) {
+    K = 32 / f;
+    g = lane / f;
+    c = lane - g * f;
+    if (g >= K) g = -1;  // spare lanes
+  } else {
+    K = 1;
+    g = 0;
+    c = lane;
+  }
+  const int nchunks = f <= 32 ? 1 : (f + 31) / 32;
+  for (int64_t pb = p0 + (int64_t)warp * K; pb < p1; pb += (int64_t)kLeafWarps * K) {
+    const int64_t p = pb + (g < 0 ? 0 : g);
+    const bool have = g >= 0 && p < p1;
+    const int64_t first = p * f;  // the parent's first child slot
+    const int glen = have ? (int)min((int64_t)f, n - first) : 0;
+    float a = 0.f, b = 0.f, cc = 0.f, d = 0.f;
+    for (int ch = 0; ch < nchunks; ch++) {
+      const int k = ch * 32 + c;  // child index within the parent
+      const int clen = glen - ch * 32;  // children of this parent from this chunk on
+      const bool valid = have && k < glen;
+      float x0 = 0.f, y0 = 0.f, x1 = 0.f, y1 = 0.f;
+      if (valid) {
+        const Box32 r = s_rec[(int)(first + k - c0)];
+        x0 = r.mbr.x;
+        y0 = r.mbr.y;
+        x1 = r.mbr.z;
+        y1 = r.mbr.w;
+        const int64_t s = first + k;
+        __stcs(oxmin + s, x0);
+        __stcs(oymin + s, y0);
+        __stcs(oxmax + s, x1);
+        __stcs(oymax + s, y1);
+        __stcs(oid + s, r.idp.x);
+      }
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const float u0 = __shfl_down_sync(0xffffffffu, x0, off);
+        const float u1 = __shfl_down_sync(0xffffffffu, y0, off);
+        const float u2 = __shfl_down_sync(0xffffffffu, x1, off);
+        const float u3 = __shfl_down_sync(0xffffffffu, y1, off);
+        if (valid && c + off < clen) {
+          x0 = fminf(x0, u0);
+          y0 = fminf(y0, u1);
+          x1 = fmaxf(x1, u2);
+          y1 = fmaxf(y1, u3);
+        }
+      }
+      if (ch == 0) {
+        a = x0; b = y0; cc = x1; d = y1;
+      } else if (clen > 0) {
+        a = fminf(a, x0); b = fminf(b, y0); cc = fmaxf(cc, x1); d = fmaxf(d, y1);
+      }
+    }
+    if (have && c == 0) {
+      const int64_t o = parent_start + p;
+      nxmin[o] = a;
+      nymin[o] = b;
+      nxmax[o] = cc;
+      nymax[o] = d;
+      npos[o] = (int)(pos_base + first);
+      nlen[o] = glen;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 int tree_levels(int64_t n, int fanout, std::vector<int64_t>& lv)
@@ -579,32 +765,53 @@ static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 static int64_t sort_tiles(int64_t n) { return std::max<int64_t>(1, cdiv(n, kSortTile)); }
 
+// Look-back status words: one per (tile, bin) of every digit.
+static int64_t status_words_before(int digit, int64_t tiles)
+{
+  int64_t w = 0;
+  for (int d = 0; d < digit; d++) w += tiles << digit_bits(d);
+  return w;
+}
+
 size_t sort_zero_bytes(int64_t n)
 {
-  return sizeof(SortCtrl) + 4 * kBins * sizeof(uint32_t) +
-         (size_t)4 * sort_tiles(n) * kBins * sizeof(uint64_t);
+  return sizeof(SortCtrl) + (size_t)kDigits * kBins * sizeof(uint32_t) +
+         (size_t)status_words_before(kDigits, sort_tiles(n)) * sizeof(uint64_t);
 }
 SortCtrl* sort_ctrl(void* zero_block) { return (SortCtrl*)zero_block; }
 uint32_t* sort_hist(void* zero_block) { return (uint32_t*)((char*)zero_block + sizeof(SortCtrl)); }
 static uint64_t* sort_status(void* zero_block)
 {
-  return (uint64_t*)((char*)zero_block + sizeof(SortCtrl) + 4 * kBins * sizeof(uint32_t));
+  return (uint64_t*)((char*)zero_block + sizeof(SortCtrl) + (size_t)kDigits * kBins * sizeof(uint32_t));
+}
+
+template <int kBits>
+static void launch_pass(int d, SortBufs bufs, int64_t n, uint64_t* status, SortCtrl* ctrl,
+                        int flags, cudaStream_t stream)
+{
+  const size_t smem = SweepSmem<kBits>::kBytes;
+  cudaFuncSetAttribute(onesweep_kernel<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  onesweep_kernel<kBits><<<(unsigned)sort_tiles(n), kSortThreads, smem, stream>>>(d, bufs, n, status,
+                                                                                  ctrl, flags);
 }
 
 void sort_passes(SortBufs bufs, int64_t n, void* zero_block, cudaStream_t stream, int flags)
 {
   const int64_t ntiles = sort_tiles(n);
   SortCtrl* ctrl = sort_ctrl(zero_block);
-  uint64_t* status = sort_status(zero_block);
-  plan_kernel<<<1, 128, 0, stream>>>(sort_hist(zero_block), n, ctrl);
-  const size_t smem = kSortSmem;
-  cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  for (int d = 0; d < 4; d++) {
+  plan_kernel<<<1, 32 * kDigits, 0, stream>>>(sort_hist(zero_block), n, ctrl);
+  for (int d = 0; d < kDigits; d++) {
     ProfScope ps("sort_pass", stream);
-    onesweep_kernel<<<(unsigned)ntiles, kSortThreads, smem, stream>>>(
-        d, bufs, n, status + (size_t)d * ntiles * kBins, ctrl, flags);
+    uint64_t* status = sort_status(zero_block) + status_words_before(d, ntiles);
+    switch (digit_bits(d)) {
+      case 10: launch_pass<10>(d, bufs, n, status, ctrl, flags, stream); break;
+      case 8: launch_pass<8>(d, bufs, n, status, ctrl, flags, stream); break;
+      case 2: launch_pass<2>(d, bufs, n, status, ctrl, flags, stream); break;
+      default: launch_pass<kDigitBits>(d, bufs, n, status, ctrl, flags, stream); break;
+    }
   }
-  CRT_LAUNCHED(5);
+  CRT_LAUNCHED(1 + kDigits);
 }
 
 // Builds the tree of `n` boxes.  in_* may alias out_* (in-place build).
@@ -676,7 +883,17 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
       int npc = (int)std::max<int64_t>(1, std::min<int64_t>(kLevelThreads, kLevelChunk / fanout));
       unsigned g = (unsigned)cdiv(np, npc);
       ProfScope ps("level", stream);
-      if (l == 0)
+      if (l == 0 && fanout <= kLeafChunk) {
+        const int ppc = kLeafChunk / fanout;
+        const size_t smem = (size_t)kLeafChunk * sizeof(Box32);
+        // the most shared memory per SM, so that six CTAs fit
+        cudaFuncSetAttribute(leaf_gather_kernel<kLeafChunk>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        leaf_gather_kernel<kLeafChunk><<<(unsigned)cdiv(np, ppc), kLeafThreads, smem, stream>>>(
+            fanout, ppc, n, np, parent_start, rsz, bufs.vals[0], bufs.vals[1], ctrl, aos, out_xmin,
+            out_ymin, out_xmax, out_ymax, out_id, nxmin, nymin, nxmax, nymax, npos, nlen);
+      } else if (l == 0)
         level_kernel<true><<<g, kLevelThreads, 0, stream>>>(
             npc, fanout, nchild, np, parent_start, rsz, bufs.vals[0], bufs.vals[1], ctrl, aos,
             out_xmin, out_ymin, out_xmax, out_ymax, out_id, nxmin, nymin, nxmax, nymax, npos,

@@ -17,21 +17,19 @@ __global__ void canon_stage_kernel(const int32_t* __restrict__ key_src,
                                    uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
                                    uint32_t* __restrict__ hist)
 {
-  __shared__ uint32_t sh[4][kBins];
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
+  __shared__ uint32_t sh[kDigits][kBins];
+  for (int i = threadIdx.x; i < kDigits * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const uint32_t k = (uint32_t)key_src[i] ^ 0x80000000u;
     keys[i] = k;
     vals[i] = (uint32_t)val_src[i];
-    atomicAdd(&sh[0][k & 0xFF], 1u);
-    atomicAdd(&sh[1][(k >> 8) & 0xFF], 1u);
-    atomicAdd(&sh[2][(k >> 16) & 0xFF], 1u);
-    atomicAdd(&sh[3][k >> 24], 1u);
+#pragma unroll
+    for (int d = 0; d < kDigits; d++) atomicAdd(&sh[d][key_digit(k, d)], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) {
+  for (int i = threadIdx.x; i < kDigits * kBins; i += blockDim.x) {
     const uint32_t v = (&sh[0][0])[i];
     if (v) atomicAdd(&hist[i], v);
   }
@@ -113,7 +111,9 @@ constexpr int kDigestRun = 64;  // consecutive pairs per thread
 // Each thread sums the pairs of its run window by window and adds each
 // window's count and digest with one pair of atomics; when every lane of a
 // warp saw one window only (the long runs of a batch query's output), the
-// warp adds once.
+// warp adds once.  Pairs are read through L2 only (ld.global.cg): they may
+// come from a kernel still running on another stream, such as the serving
+// loop, whose completed requests this checks.
 __global__ void __launch_bounds__(256)
     digest_kernel(const int32_t* __restrict__ fid, const int32_t* __restrict__ tid, int64_t n,
                   int64_t base, int64_t nq, unsigned long long* __restrict__ counts,
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256)
     unsigned long long c = 0, h = 0, nbad = 0;
     bool single = true;  // the whole run is one window
     for (int64_t i = i0; i < i1; i++) {
-      const long long w = (long long)__ldg(tid + i) + base;
+      const long long w = (long long)__ldcg(tid + i) + base;
       if (w < 0 || w >= nq) {
         nbad++;
         single = false;
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(256)
         h = 0;
       }
       c++;
-      h += pair_mix(((unsigned long long)(uint32_t)w << 32) | (uint32_t)__ldg(fid + i));
+      h += pair_mix(((unsigned long long)(uint32_t)w << 32) | (uint32_t)__ldcg(fid + i));
     }
     // warp aggregation: all lanes hold one segment of the same window
     const long long w0 = __shfl_sync(0xffffffffu, cur, 0);

@@ -322,8 +322,9 @@ __device__ __forceinline__ int64_t float_field(const uint8_t* t, int64_t p, floa
 }
 
 // An integer field at p: the low 32 bits of its value (what (int) of strtol
-// keeps); the last field may be followed by ' '/'\t' and ends at ',', '\n'
-// or '\r'; the others end at ','.
+// keeps); the others end at ','; the last one may be followed by ' ', '\t'
+// or '\r' and must end its line (the fast path takes one record per line:
+// then the next record starts on the next line, as fscanf finds it).
 __device__ __forceinline__ int64_t int_field(const uint8_t* t, int64_t p, bool last, int32_t* v)
 {
   const int64_t p0 = p, lim = p + kFieldMax;
@@ -339,9 +340,9 @@ __device__ __forceinline__ int64_t int_field(const uint8_t* t, int64_t p, bool l
   }
   if (nd == 0 || nd > 18) return -1;
   if (last)
-    while (p < lim && (c == ' ' || c == '\t')) c = at(t, ++p);
+    while (p < lim && (c == ' ' || c == '\t' || c == '\r')) c = at(t, ++p);
   if (p - p0 > kFieldMax) return -1;
-  if (last ? !(c == ',' || c == '\n' || c == '\r') : c != ',') return -1;
+  if (last ? c != '\n' : c != ',') return -1;
   *v = (int32_t)(uint32_t)(neg ? 0 - x : x);
   return p;
 }
@@ -406,10 +407,14 @@ __global__ void __launch_bounds__(kParseThreads, 4)
       ymax[k] = add_host(v[1] < v[3] ? v[3] : v[1], r);
       id[k] = rid;
     } else {
+      // for the host parser: the record, its start, and the next record's
+      // start (-1 for the last), against which the host checks where the
+      // record really ends
       const unsigned long long j = atomicAdd(n_fallback, 1ull);
       if ((int64_t)j < fallback_cap) {
-        fallback[2 * j] = k;
-        fallback[2 * j + 1] = s;
+        fallback[3 * j] = k;
+        fallback[3 * j + 1] = s;
+        fallback[3 * j + 2] = k + 1 < m ? starts[k + 1] : -1;
       }
     }
   }
@@ -656,7 +661,7 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
     CRT_CUDA(cudaStreamSynchronize(stream));
   }
   const int64_t total = (int64_t)h_ctr[0];
-  const int64_t m = n < 0 ? total : std::min(total, n);
+  int64_t m = n < 0 ? total : std::min(total, n);
   if (alloc) {
     if (m > INT32_MAX) return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv_device: more than 2^31-1 records");
     void** dst[5] = {(void**)&out.xmin, (void**)&out.ymin, (void**)&out.xmax, (void**)&out.ymax,
@@ -680,7 +685,7 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
   if (m > 0) {
     const int64_t cap = std::min(m, kFallbackCap);
     int64_t* starts = S.get<int64_t>((size_t)m * 8);
-    int64_t* fb = S.get<int64_t>((size_t)cap * 16);
+    int64_t* fb = S.get<int64_t>((size_t)cap * 24);
     if (!starts || !fb) {
       release();
       return fail(CRT_ERR_OOM, "read_mbr_csv_device: device allocation failed");
@@ -712,54 +717,81 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
         release();
         return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv_device: reading the file failed");
       }
+      const char* end = base + src.len;
       std::vector<FixRecord> fix;
-      if (c > cap) {
-        // too many for the list: the host loader parses every record
-        std::vector<float> hv[4];
-        for (auto& v : hv) v.resize((size_t)m);
-        std::vector<int32_t> hid((size_t)m);
-        int64_t got = 0;
-        rc = read_mbr_text(base, (size_t)src.len, m, r, hv[0].data(), hv[1].data(), hv[2].data(),
-                           hv[3].data(), hid.data(), &got);
-        if (rc != CRT_OK) first_bad = got;
-        const size_t bytes = (size_t)(first_bad >= 0 ? first_bad : m) * 4;
-        float* dv[4] = {out.xmin, out.ymin, out.xmax, out.ymax};
-        for (int a = 0; a < 4 && bytes && e == cudaSuccess; a++)
-          e = cudaMemcpy(dv[a], hv[a].data(), bytes, cudaMemcpyHostToDevice);
-        if (bytes && e == cudaSuccess) e = cudaMemcpy(out.id, hid.data(), bytes, cudaMemcpyHostToDevice);
-      } else {
-        std::vector<int64_t> h_fb((size_t)c * 2);
-        e = cudaMemcpy(h_fb.data(), fb, (size_t)c * 16, cudaMemcpyDeviceToHost);
-        const char* end = base + src.len;
-        for (int64_t j = 0; j < c && e == cudaSuccess; j++) {
-          const int64_t k = h_fb[2 * j], s = h_fb[2 * j + 1];
+      bool whole = c > cap;  // too many for the list: the host loader reads the file
+      if (!whole) {
+        std::vector<int64_t> h_fb((size_t)c * 3);
+        e = cudaMemcpy(h_fb.data(), fb, (size_t)c * 24, cudaMemcpyDeviceToHost);
+        for (int64_t j = 0; j < c && e == cudaSuccess && !whole; j++) {
+          const int64_t k = h_fb[3 * j], s0 = h_fb[3 * j + 1], next = h_fb[3 * j + 2];
           float v[4];
           int rid = 0;
-          if (!parse_mbr_record(base + s, end, v, rid)) {
+          const char* stop = parse_mbr_record(base + s0, end, v, rid);
+          if (!stop) {
             if (first_bad < 0 || k < first_bad) first_bad = k;
             continue;
+          }
+          // a record that does not end where the line scan put the next one
+          // (records across lines, several on a line): fscanf's records are
+          // not the lines here, so the host loader reads the whole file
+          if (next >= 0 ? stop != base + next : (m < n || n < 0) && stop != end) {
+            whole = true;
+            break;
           }
           FixRecord f{k, 0, 0, 0, 0, rid, 0};
           mbr_box(v, r, &f.xmin, &f.ymin, &f.xmax, &f.ymax);
           fix.push_back(f);
         }
-        if (!fix.empty() && e == cudaSuccess) {
-          FixRecord* d_fix = S.get<FixRecord>(fix.size() * sizeof(FixRecord));
-          if (!d_fix) {
-            release();
-            return fail(CRT_ERR_OOM, "read_mbr_csv_device: device allocation failed");
-          }
-          e = cudaMemcpyAsync(d_fix, fix.data(), fix.size() * sizeof(FixRecord),
-                              cudaMemcpyHostToDevice, stream);
-          const int64_t g = std::min<int64_t>(cdiv((int64_t)fix.size(), 256), (int64_t)sm_count() * 4);
-          if (e == cudaSuccess) {
-            mbr_fix_kernel<<<(unsigned)g, 256, 0, stream>>>(d_fix, (int64_t)fix.size(), out.xmin,
-                                                           out.ymin, out.xmax, out.ymax, out.id);
-            CRT_LAUNCHED(1);
-            e = cudaGetLastError();
-          }
-          if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      }
+      if (whole && e == cudaSuccess) {
+        MbrRecords rec;
+        scan_mbr_text(base, (size_t)src.len, n, r, rec);
+        first_bad = rec.malformed || (n >= 0 && rec.count < n) ? rec.count : -1;
+        if (first_bad < 0 && rec.count != m && !alloc) {
+          m = rec.count;  // the caller's arrays hold n >= rec.count records
+        } else if (first_bad < 0 && rec.count != m) {
+          // fscanf finds another number of records than the line scan
+          release();
+          m = rec.count;
+          if (m > INT32_MAX)
+            return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv_device: more than 2^31-1 records");
+          void** dst[5] = {(void**)&out.xmin, (void**)&out.ymin, (void**)&out.xmax,
+                           (void**)&out.ymax, (void**)&out.id};
+          for (int a2 = 0; a2 < 5; a2++) *dst[a2] = nullptr;
+          for (int a2 = 0; a2 < 5 && m > 0; a2++)
+            if (cudaMalloc(dst[a2], (size_t)m * 4) != cudaSuccess) {
+              cudaGetLastError();
+              for (int b2 = 0; b2 < a2; b2++) cudaFree(*dst[b2]);
+              return fail(CRT_ERR_OOM, "read_mbr_csv_device: output allocation failed");
+            }
         }
+        const size_t bytes = (size_t)std::min<int64_t>(rec.count, m) * 4;
+        float* dv[4] = {out.xmin, out.ymin, out.xmax, out.ymax};
+        for (int a2 = 0; a2 < 4 && bytes && e == cudaSuccess; a2++)
+          e = cudaMemcpy(dv[a2], rec.v[a2].data(), bytes, cudaMemcpyHostToDevice);
+        if (bytes && e == cudaSuccess) e = cudaMemcpy(out.id, rec.id.data(), bytes, cudaMemcpyHostToDevice);
+        if (first_bad >= 0 && !rec.malformed) {
+          // fewer records than asked for: reported below with the count
+          first_bad = -1;
+          m = rec.count;
+        }
+      } else if (!fix.empty() && e == cudaSuccess) {
+        FixRecord* d_fix = S.get<FixRecord>(fix.size() * sizeof(FixRecord));
+        if (!d_fix) {
+          release();
+          return fail(CRT_ERR_OOM, "read_mbr_csv_device: device allocation failed");
+        }
+        e = cudaMemcpyAsync(d_fix, fix.data(), fix.size() * sizeof(FixRecord),
+                            cudaMemcpyHostToDevice, stream);
+        const int64_t g = std::min<int64_t>(cdiv((int64_t)fix.size(), 256), (int64_t)sm_count() * 4);
+        if (e == cudaSuccess) {
+          mbr_fix_kernel<<<(unsigned)g, 256, 0, stream>>>(d_fix, (int64_t)fix.size(), out.xmin,
+                                                         out.ymin, out.xmax, out.ymax, out.id);
+          CRT_LAUNCHED(1);
+          e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
       }
       if (e != cudaSuccess) {
         release();

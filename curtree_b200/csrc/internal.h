@@ -16,8 +16,28 @@ struct SortBufs {
   uint32_t* vals[2];
 };
 
-constexpr int kBins = 256;
+// Radix digits of the 32-bit sort keys: kDigits digits of kDigitBits bits
+// from the least significant end, the last one narrower (10 + 10 + 10 + 2:
+// keys whose top two bits never vary -- every Morton key of coordinates in
+// [0, 2^15) -- sort in three passes).  Histograms and bucket starts keep
+// kBins entries per digit.
+#ifndef CRT_SORT_DIGIT_BITS
+#define CRT_SORT_DIGIT_BITS 10
+#endif
+constexpr int kDigitBits = CRT_SORT_DIGIT_BITS;
+constexpr int kBins = 1 << kDigitBits;
+constexpr int kDigits = (32 + kDigitBits - 1) / kDigitBits;
+static_assert(kDigits == 4, "four digit passes at most");
 constexpr int kSortTile = 8192;
+
+__host__ __device__ constexpr int digit_bits(int d)
+{
+  return 32 - d * kDigitBits < kDigitBits ? 32 - d * kDigitBits : kDigitBits;
+}
+__device__ __forceinline__ uint32_t key_digit(uint32_t k, int d)
+{
+  return (k >> (d * kDigitBits)) & ((1u << digit_bits(d)) - 1u);
+}
 
 // Control block of one sort (int32 words, zero-initialised by the caller).
 struct SortCtrl {
@@ -26,11 +46,12 @@ struct SortCtrl {
   int active;       // bit d: digit d is non-uniform
   int n_active;     // number of active passes: the order is in vals[n_active & 1]
   int pad[9];
-  int bucket_start[4 * kBins];
+  int bucket_start[kDigits * kBins];
 };
 
-// Bytes of zero-initialised state a sort of n keys needs: SortCtrl, the four
-// digit histograms and the look-back status words (in that order).
+// Bytes of zero-initialised state a sort of n keys needs: SortCtrl, the
+// digit histograms (kDigits x kBins words, filled by the caller's key kernel
+// with key_digit) and the look-back status words (in that order).
 size_t sort_zero_bytes(int64_t n);
 // Enqueues plan + four onesweep passes; keys must be in bufs.keys[0] and the
 // histograms filled.  The sorted positions end in bufs.vals[n_active & 1]
@@ -63,11 +84,23 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
                int64_t* d_offsets, const crt_query_opts& opts, cudaStream_t stream);
 int64_t query_capacity(int64_t pairs, const crt_query_opts& opts);
 
-// Host parser of the reference's MBR text format (io.cu): one record at p
-// (false if malformed), the box readMBR makes of its four numbers, and the
-// whole loader over text in memory (statuses and *n_read as crt_read_mbr_csv).
-bool parse_mbr_record(const char* p, const char* end, float v[4], int& id);
+// Host parser of the reference's MBR text format (io.cu), with the rules of
+// readMBR's fscanf(fp, "%f,%f,%f,%f,%d,%d,%d\n", ...): one record at p (the
+// position after it and the whitespace that follows, or nullptr where fscanf
+// reads fewer than seven fields), the box readMBR makes of its four numbers,
+// and whole texts: scan_mbr_text reads up to `limit` records (limit < 0:
+// all) in fscanf's order, stopping at the end of the text or at a malformed
+// record; read_mbr_text does so into caller arrays (statuses and *n_read as
+// crt_read_mbr_csv).
+const char* parse_mbr_record(const char* p, const char* end, float v[4], int& id);
 void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, float* ymax);
+struct MbrRecords {
+  std::vector<float> v[4];  // xmin, ymin, xmax, ymax
+  std::vector<int32_t> id;
+  int64_t count = 0;
+  bool malformed = false;  // stopped at a record fscanf cannot read
+};
+void scan_mbr_text(const char* base, size_t len, int64_t limit, float r, MbrRecords& out);
 int read_mbr_text(const char* base, size_t len, int64_t n, float r, float* xmin, float* ymin,
                   float* xmax, float* ymax, int32_t* id, int64_t* n_read);
 

@@ -1,15 +1,16 @@
 // Host-side I/O around the tree: the reference's MBR text loader and a tree
 // file format.
 //
-// crt_read_mbr_csv restates readMBR (src/utility.cpp:5-40): each record is a
-// line "x1,y1,x2,y2,id,pid,nume"; the box is [min(x1,x2) - r, max(x1,x2) + r]
-// x [min(y1,y2) - r, max(y1,y2) + r] in fp32, id is the fifth field, pid and
-// nume are read and dropped.  Numbers parse as fscanf's %f / %d do (strtof /
-// strtol, correctly rounded); blanks may precede a number and end a line, but
-// not precede a ',' (the format's literal commas do not skip blanks); one
-// record per line, blank lines skipped.  Where the
-// reference exits (missing file) or throws (a malformed record), this
-// returns a status.  Records are parsed by several host threads.
+// crt_read_mbr_csv restates readMBR (src/utility.cpp:5-40), which reads each
+// record with fscanf(fp, "%f,%f,%f,%f,%d,%d,%d\n", ...): the box is
+// [min(x1,x2) - r, max(x1,x2) + r] x [min(y1,y2) - r, max(y1,y2) + r] in fp32,
+// id is the fifth field, pid and nume are read and dropped.  Numbers parse as
+// fscanf's %f / %d do (strtof / strtol, correctly rounded); whitespace
+// (newlines included) may precede a number but not a ',' (the format's
+// literal commas do not skip it), and the closing "\n" skips any whitespace,
+// so records need not sit one per line.  Where the reference exits (missing
+// file) or throws (a malformed record), this returns a status.  Records are
+// parsed by several host threads.
 //
 // crt_tree_save / crt_tree_load write and read a built tree with its sorted
 // box set, a format the reference does not have:
@@ -51,87 +52,108 @@ bool read_file(const char* path, std::string& out)
   return ok;
 }
 
+// fscanf's whitespace (isspace in the C locale)
+inline bool is_space(char c)
+{
+  return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
+}
+
 inline const char* skip_ws(const char* p, const char* end)
 {
-  while (p < end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) p++;
+  while (p < end && is_space(*p)) p++;
   return p;
 }
 
 }  // namespace
 
-// One record "x1,y1,x2,y2,id,pid,nume" starting at p; false if malformed.
-bool parse_mbr_record(const char* p, const char* end, float v[4], int& id)
+// One record of readMBR's fscanf(fp, "%f,%f,%f,%f,%d,%d,%d\n", ...) at p:
+// each number may be preceded by whitespace (newlines too); the literal ','
+// must follow a number at once; after the last number the format's closing
+// "\n" skips any whitespace, and whatever follows begins the next record.
+// Returns the position after the record and that whitespace, or nullptr
+// where fscanf would read fewer than seven fields.
+const char* parse_mbr_record(const char* p, const char* end, float v[4], int& id)
 {
   char buf[64];
+  std::string big;
   for (int f = 0; f < 7; f++) {
     p = skip_ws(p, end);
     size_t m = 0;
-    while (p + m < end && p[m] != ',' && p[m] != '\n' && p[m] != '\r' && m < sizeof(buf) - 1) m++;
-    if (m == 0) return false;
-    std::memcpy(buf, p, m);
-    buf[m] = 0;
-    char* stop = nullptr;
-    errno = 0;
-    if (f < 4) {
-      v[f] = std::strtof(buf, &stop);
+    while (p + m < end && p[m] != ',' && !is_space(p[m])) m++;
+    if (m == 0) return nullptr;
+    const char* tok = buf;
+    if (m < sizeof(buf)) {
+      std::memcpy(buf, p, m);
+      buf[m] = 0;
     } else {
-      const long x = std::strtol(buf, &stop, 10);
+      big.assign(p, m);
+      tok = big.c_str();
+    }
+    char* stop = nullptr;
+    if (f < 4) {
+      v[f] = std::strtof(tok, &stop);
+    } else {
+      const long x = std::strtol(tok, &stop, 10);
       if (f == 4) id = (int)x;
     }
-    // fscanf skips blanks before a number, and the format's closing newline
-    // matches blanks after the last one; a blank before a ',' fails the match
-    if (f == 6)
-      while (stop && (*stop == ' ' || *stop == '\t')) stop++;
-    if (!stop || *stop != 0) return false;
-    p += m;
+    if (!stop || stop == tok) return nullptr;  // no number here
+    const size_t used = (size_t)(stop - tok);
     if (f < 6) {
-      if (p >= end || *p != ',') return false;
-      p++;
+      if (used != m || p + m >= end || p[m] != ',') return nullptr;
+      p += m + 1;
+    } else {
+      p += used;
     }
   }
-  return true;
+  return skip_ws(p, end);
 }
 
 namespace {
 
-// Class of a stretch's last byte that is not ' ', '\t' or '\r'.
-constexpr int kNoByte = 0, kNewline = 1, kOtherByte = 2;
-
-inline bool is_blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
+// Class of a stretch's last byte that is not whitespace.
+constexpr int kNoByte = 0, kComma = 1, kOtherByte = 2;
 
 int last_class(const char* p, const char* e)
 {
   while (e > p) {
     const char c = *--e;
-    if (!is_blank(c)) return c == '\n' ? kNewline : kOtherByte;
+    if (!is_space(c)) return c == ',' ? kComma : kOtherByte;
   }
   return kNoByte;
 }
 
-// Record starts in [b, e), at most `cap`, given the class of the last
-// non-blank byte before b.
+// Candidate record starts in [b, e), at most `cap`: a byte that is neither
+// whitespace nor ',' whose previous byte is whitespace (or absent) and whose
+// last non-whitespace predecessor is not a ',' (or absent).  `in` is the
+// class of the last non-whitespace byte before b.
 void chunk_starts(const char* base, size_t b, size_t e, int in, int64_t cap,
                   std::vector<size_t>& out)
 {
   int prev = in;
+  bool ws = b == 0 || is_space(base[b - 1]);
   for (size_t i = b; i < e && (int64_t)out.size() < cap; i++) {
     const char c = base[i];
-    if (is_blank(c)) continue;
-    if (c != '\n' && prev != kOtherByte) out.push_back(i);
-    prev = c == '\n' ? kNewline : kOtherByte;
+    if (is_space(c)) {
+      ws = true;
+      continue;
+    }
+    if (c != ',' && ws && prev != kComma) out.push_back(i);
+    prev = c == ',' ? kComma : kOtherByte;
+    ws = false;
   }
 }
 
 }  // namespace
 
-// The first n record starts: the first byte of each line that is not ' ',
-// '\t' or '\r', unless it is the line's '\n' -- the same as "a byte that is
-// neither blank nor '\n' whose previous non-blank byte is a '\n' or absent".
-// The second form splits: host threads take 8 MiB chunks, the class each
-// chunk ends with is carried across the chunks, then each thread lists its
-// chunk's starts.
+// The first n candidate record starts (n < 0: all).  In a text that fscanf
+// reads record after record, these are where its records begin: every
+// record's first number follows whitespace (or begins the text), and no
+// other number is both preceded by whitespace and not preceded by a ','.
+// Host threads take 8 MiB chunks; the class each chunk ends with is carried
+// across the chunks, then each thread lists its chunk's starts.
 std::vector<size_t> record_starts(const char* base, size_t L, int64_t n)
 {
+  if (n < 0) n = INT64_MAX;
   constexpr size_t kChunk = size_t(8) << 20;
   const int hw = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   const int nt = (int)std::max<size_t>(1, std::min<size_t>((size_t)hw, (L + kChunk - 1) / kChunk));
@@ -156,7 +178,6 @@ std::vector<size_t> record_starts(const char* base, size_t L, int64_t n)
     chunk_starts(base, b, e, in, n, part[t]);
   });
   std::vector<size_t> starts;
-  starts.reserve((size_t)std::max<int64_t>(0, n));
   for (int t = 0; t < nt && (int64_t)starts.size() < n; t++) {
     const size_t take = (size_t)std::min<int64_t>((int64_t)part[t].size(), n - (int64_t)starts.size());
     starts.insert(starts.end(), part[t].begin(), part[t].begin() + take);
@@ -173,14 +194,22 @@ void mbr_box(const float v[4], float r, float* xmin, float* ymin, float* xmax, f
   *ymax = std::max(v[1], v[3]) + r;
 }
 
-int read_mbr_text(const char* base, size_t L, int64_t n, float r, float* xmin, float* ymin,
-                  float* xmax, float* ymax, int32_t* id, int64_t* n_read)
+// Records in readMBR's order: the candidate starts are parsed by host
+// threads, and the records are kept up to the first one that does not begin
+// exactly where the one before ended (after its trailing whitespace) or does
+// not parse; from there the text is read one record after another, as
+// fscanf reads it.  So the result is fscanf's for any text, and parallel for
+// the usual one: records separated by whitespace, no record ending in a
+// byte that runs into the next number.
+void scan_mbr_text(const char* base, size_t L, int64_t limit, float r, MbrRecords& out)
 {
-  const std::vector<size_t> starts = record_starts(base, L, n);
-  const int64_t m = (int64_t)starts.size();
   const char* end = base + L;
-  int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  std::vector<int64_t> bad(nt, -1);
+  const std::vector<size_t> starts = record_starts(base, L, limit);
+  const int64_t m = (int64_t)starts.size();
+  for (auto& v : out.v) v.resize((size_t)m);
+  out.id.resize((size_t)m);
+  std::vector<int64_t> ends((size_t)m, -1);
+  const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   std::vector<std::thread> th;
   const int64_t per = (m + nt - 1) / nt;
   for (int t = 0; t < nt; t++) {
@@ -188,25 +217,58 @@ int read_mbr_text(const char* base, size_t L, int64_t n, float r, float* xmin, f
       for (int64_t k = t * per; k < std::min(m, (t + 1) * per); k++) {
         float v[4];
         int rid = 0;
-        if (!parse_mbr_record(base + starts[k], end, v, rid)) {
-          bad[t] = k;
-          return;
-        }
-        mbr_box(v, r, &xmin[k], &ymin[k], &xmax[k], &ymax[k]);
-        id[k] = rid;
+        const char* e = parse_mbr_record(base + starts[k], end, v, rid);
+        if (!e) continue;
+        ends[k] = e - base;
+        mbr_box(v, r, &out.v[0][k], &out.v[1][k], &out.v[2][k], &out.v[3][k]);
+        out.id[k] = rid;
       }
     });
   }
   for (auto& x : th) x.join();
-  int64_t first_bad = -1;
-  for (auto b : bad)
-    if (b >= 0 && (first_bad < 0 || b < first_bad)) first_bad = b;
-  if (first_bad >= 0) {
-    if (n_read) *n_read = first_bad;
-    return fail(CRT_ERR_INVALID_ARG,
-                "read_mbr_csv: record " + std::to_string(first_bad) + " is not x1,y1,x2,y2,id,pid,nume");
+  // keep the records fscanf would read the same way
+  int64_t expect = skip_ws(base, end) - base;
+  int64_t good = 0;
+  while (good < m && (int64_t)starts[good] == expect && ends[good] >= 0) expect = ends[good++];
+  for (auto& v : out.v) v.resize((size_t)good);
+  out.id.resize((size_t)good);
+  out.count = good;
+  out.malformed = false;
+  // then one record after another from where the last kept one ended
+  const char* p = base + expect;
+  while (limit < 0 || out.count < limit) {
+    p = skip_ws(p, end);
+    if (p >= end) break;  // end of text: fewer records than asked for
+    float v[4];
+    int rid = 0;
+    const char* e = parse_mbr_record(p, end, v, rid);
+    if (!e) {
+      out.malformed = true;
+      break;
+    }
+    float b[4];
+    mbr_box(v, r, &b[0], &b[1], &b[2], &b[3]);
+    for (int a = 0; a < 4; a++) out.v[a].push_back(b[a]);
+    out.id.push_back(rid);
+    out.count++;
+    p = e;
   }
+}
+
+int read_mbr_text(const char* base, size_t L, int64_t n, float r, float* xmin, float* ymin,
+                  float* xmax, float* ymax, int32_t* id, int64_t* n_read)
+{
+  MbrRecords rec;
+  scan_mbr_text(base, L, n, r, rec);
+  const int64_t m = rec.count;
+  float* dst[4] = {xmin, ymin, xmax, ymax};
+  for (int a = 0; a < 4; a++)
+    if (m) std::memcpy(dst[a], rec.v[a].data(), sizeof(float) * (size_t)m);
+  if (m) std::memcpy(id, rec.id.data(), sizeof(int32_t) * (size_t)m);
   if (n_read) *n_read = m;
+  if (rec.malformed)
+    return fail(CRT_ERR_INVALID_ARG,
+                "read_mbr_csv: record " + std::to_string(m) + " is not x1,y1,x2,y2,id,pid,nume");
   if (m < n)
     return fail(CRT_ERR_INVALID_ARG, "read_mbr_csv: file holds " + std::to_string(m) +
                                          " records, " + std::to_string(n) + " requested");

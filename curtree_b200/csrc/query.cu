@@ -742,20 +742,18 @@ __global__ void __launch_bounds__(256)
 __global__ void window_key_kernel(WindowView W, uint32_t* __restrict__ keys,
                                   uint32_t* __restrict__ hist)
 {
-  __shared__ uint32_t sh[4][kBins];
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
+  __shared__ uint32_t sh[kDigits][kBins];
+  for (int i = threadIdx.x; i < kDigits * kBins; i += blockDim.x) (&sh[0][0])[i] = 0;
   __syncthreads();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < W.n;
        i += (long long)gridDim.x * blockDim.x) {
     uint32_t k = sort_key(W.xmin[i], W.ymin[i], W.xmax[i], W.ymax[i]);
     keys[i] = k;
-    atomicAdd(&sh[0][k & 0xFF], 1u);
-    atomicAdd(&sh[1][(k >> 8) & 0xFF], 1u);
-    atomicAdd(&sh[2][(k >> 16) & 0xFF], 1u);
-    atomicAdd(&sh[3][k >> 24], 1u);
+#pragma unroll
+    for (int d = 0; d < kDigits; d++) atomicAdd(&sh[d][key_digit(k, d)], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 4 * kBins; i += blockDim.x) {
+  for (int i = threadIdx.x; i < kDigits * kBins; i += blockDim.x) {
     uint32_t v = (&sh[0][0])[i];
     if (v) atomicAdd(&hist[i], v);
   }

@@ -198,6 +198,18 @@ LAYOUT_CASES = [
     "1..2,2,3,4,5,6,7\n",
     "1,2,3,4,-,6,7\n",
     "\r\r\r1,2,3,4,5,6,7\r\r\n",
+    # fscanf's records are not the lines: across lines, several on a line,
+    # whatever follows the seventh number starting the next record
+    "1,2,\n3,4,5,6,7\n8,9,10,11,12,13,14\n",
+    "1,2,3,4,5,6,7 8,9,10,11,12,13,14\n",
+    "1,2,3,4,5,6,7\t\v\f8,9,10,11,12,13,14",
+    "1,2,3,4,5,6,7,8\n9,9,9,9,9,9,9\n",
+    "1,2,3,4,5,6,7x\n8,9,10,11,12,13,14\n",
+    "1,2,3,4,5,6,7-8,9,10,11,12,13,14\n",
+    "1,\n2,\n3,\n4,\n5,\n6,\n7\n",
+    "1.5e3,2,3,4,5,6,7 8,9,10,11,12,13,14 15,16,17,18,19,20,21",
+    "1,2,3,4\n,5,6,7\n",
+    "1,2,3,4,5,6,7\r8,9,10,11,12,13,14\n",
 ]
 
 
@@ -409,3 +421,24 @@ def test_binary_and_text_forms_agree(crt):
         for u, v in zip((x.xmin, x.ymin, x.xmax, x.ymax), (y.xmin, y.ymin, y.xmax, y.ymax)):
             assert np.array_equal(u.view(np.uint32), v.view(np.uint32))
         assert np.array_equal(x.id, b.id) and np.array_equal(y.id, b.id)
+
+
+def test_read_all_records_as_fscanf_finds_them(crt):
+    """n = -1 (every record of the file): where fscanf's records are not the
+    lines, the device loader returns the host loader's records all the same,
+    and as many of them."""
+    texts = [c for c in LAYOUT_CASES if c.count(",") >= 6]
+    with tempfile.TemporaryDirectory() as tmp:
+        for text in texts:
+            path = os.path.join(tmp, "t.csv")
+            with open(path, "wb") as f:
+                f.write(text.encode("latin-1"))
+            hs, hn, ha, hi = host_read(path, 64, 0.5)  # 64 > any record count here
+            ds, dn, da, di = device_read(path, -1, 0.5)
+            if ds == _lib.CRT_OK:
+                assert dn == hn, text
+                for x, y in zip(ha, da):
+                    assert np.array_equal(x[:hn].view(np.uint32), y.view(np.uint32)), text
+                assert np.array_equal(hi[:hn], di), text
+            else:
+                assert ds == _lib.CRT_ERR_INVALID_ARG and dn == hn, (text, hs, hn, ds, dn)

@@ -188,3 +188,53 @@ def test_multi_chunk_file_matches_reference():
             assert np.array_equal(ids, ref.id)
         st, got, _, _ = read_ours(path, len(rows) + 1, 0.5)
         assert (st, got) == (_lib.CRT_ERR_INVALID_ARG, len(rows))
+
+
+# Texts where fscanf's records are not the lines: readMBR reads each record
+# with fscanf(fp, "%f,%f,%f,%f,%d,%d,%d\n", ...), whose numbers skip any
+# whitespace before them (newlines too) and whose closing "\n" skips any
+# whitespace after the last one -- so a record may span lines, several may
+# share a line, and what follows the seventh number starts the next record.
+FSCANF_TEXTS = [
+    ("1,2,\n3,4,5,6,7\n8,9,10,11,12,13,14\n", 2),
+    ("1,2,3,4,5,6,7 8,9,10,11,12,13,14\n", 2),
+    ("1,2,3,4,5,6,7\t\v\f8,9,10,11,12,13,14", 2),
+    ("1,2,3,4,5,6,7,8\n9,9,9,9,9,9,9\n", 2),
+    ("1,2,3,4,5,6,7x\n8,9,10,11,12,13,14\n", 2),
+    ("1,2,3,4,5,6,7-8,9,10,11,12,13,14\n", 2),
+    ("\n\n  1,2,3,4,5,6,7\n\n\n8,9,10,11,12,13,14\n\n", 2),
+    ("1,\n2,\n3,\n4,\n5,\n6,\n7\n", 1),
+    ("1.5e3,2,3,4,5,6,7 8,9,10,11,12,13,14 15,16,17,18,19,20,21", 3),
+    ("1,2,3,4,5,6,7\n", 2),
+    ("1,2,3,4\n,5,6,7\n", 1),
+]
+
+
+def ref_records(path, n):
+    """How many records the reference's readMBR reads before it throws (it
+    throws at the first record fscanf cannot read, end of file included)."""
+    for k in range(n, 0, -1):
+        try:
+            O.ref_read_mbr(path, k, 0.0)
+            return k
+        except ValueError:
+            continue
+    return 0
+
+
+@pytest.mark.skipif(not O.ref_cpu_available(), reason="reference CPU build absent")
+@pytest.mark.parametrize("text,n", FSCANF_TEXTS)
+def test_records_found_as_fscanf_finds_them(text, n):
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "t.csv")
+        with open(path, "w") as f:
+            f.write(text)
+        k = ref_records(path, n)
+        st, got, a, ids = read_ours(path, n, 0.25)
+        assert got == k
+        assert (st == _lib.CRT_OK) == (k == n)
+        if k == n:
+            ref = O.ref_read_mbr(path, n, 0.25)
+            for mine, theirs in zip(a, (ref.xmin, ref.ymin, ref.xmax, ref.ymax)):
+                assert np.array_equal(mine.view(np.uint32), theirs.view(np.uint32))
+            assert np.array_equal(ids, ref.id)
