@@ -65,7 +65,10 @@ def parse():
     p.add_argument("--fanout", type=int, default=FANOUT)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--warps", type=int, default=0, help="warps per CTA of the persistent traversal")
-    p.add_argument("--stage", type=int, default=1, help="stage the top tree levels in shared memory")
+    p.add_argument("--stage", type=int, default=2,
+                   help="whole tree levels below the root staged in shared memory")
+    p.add_argument("--window-warps", type=int, default=1, help="warps sharing one window")
+    p.add_argument("--chunk", type=int, default=4096, help="output slots a warp reserves")
     p.add_argument("--sort-windows", type=int, default=1)
     p.add_argument("--autotune", type=int, default=1, help="pick fanout/warps/staging first (untimed)")
     p.add_argument("--autotune-windows", type=int, default=100_000)
@@ -369,9 +372,12 @@ def run_ours(args, rank, world, dist):
         args.fanout = tuned["fanout"]
         args.warps = tuned["warps_per_cta"]
         args.stage = tuned["stage_levels"]
+        args.window_warps = tuned["warps_per_window"]
+        args.chunk = tuned["chunk"]
         torch.cuda.empty_cache()
     out["autotune"] = None if tuned is None else {
-        "chosen": {k: tuned[k] for k in ("fanout", "warps_per_cta", "stage_levels", "chunk", "ms")},
+        "chosen": {k: tuned[k] for k in ("fanout", "warps_per_cta", "stage_levels",
+                                         "warps_per_window", "chunk", "ms")},
         "sample_windows": int(sample.n),
         "table": [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in row.items()}
                   for row in tuned["table"]]}
@@ -380,7 +386,7 @@ def run_ours(args, rank, world, dist):
     d_win = C.BBox.from_host(windows)
     st = C.query_stats(rt, sorted_box, d_win)
     pairs, tested, tested_c = st["hits"], st["tested"], st["tested_contain"]
-    cap = C.query_capacity(pairs)
+    cap = C.query_capacity(pairs, chunk=args.chunk)
     fid = torch.empty(cap, dtype=torch.int32, device="cuda")
     tid = torch.empty(cap, dtype=torch.int32, device="cuda")
     res = C.new_result_block()
@@ -388,7 +394,8 @@ def run_ours(args, rank, world, dist):
     # ---- persistent form (graph plan) -------------------------------------
     L.crt_profile_enable(1)
     qopts = {"warps_per_cta": args.warps, "stage_levels": args.stage,
-             "sort_windows": args.sort_windows}
+             "sort_windows": args.sort_windows, "warps_per_window": args.window_warps,
+             "chunk": args.chunk}
     plan = C.Plan(rt, sorted_box, d_win, fid, tid, res, **qopts)
     for _ in range(args.warmup):
         plan.launch()

@@ -51,7 +51,7 @@ class crt_query_opts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("sort_windows", ctypes.c_int),
                 ("stage_levels", ctypes.c_int), ("warps_per_cta", ctypes.c_int),
                 ("chunk", ctypes.c_int), ("no_contain", ctypes.c_int),
-                ("reserved", ctypes.c_int * 2)]
+                ("warps_per_window", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
 
 
 class crt_query_result(ctypes.Structure):

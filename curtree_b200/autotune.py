@@ -2,8 +2,10 @@
 
 Picks, for one box set and a sample of its windows: the fanout of the tree
 (every fanout gives the same pair set; it trades tree depth against wasted
-leaf tests), the warps per CTA of the persistent traversal, whether the top
-levels are staged in shared memory, and the output chunk a warp reserves.
+leaf tests), the warps per CTA of the persistent traversal, how many whole
+tree levels are staged in shared memory, how many warps share one window,
+and the output chunk a warp reserves (the frontier itself needs no
+capacity: each warp's stack is sized exactly from the tree's depth).
 Each candidate tree is built once (out of place, so the input is untouched);
 each configuration is timed with CUDA events over a few repetitions and the
 fastest median wins.  Results are cached in a JSON file keyed by the device
@@ -28,10 +30,29 @@ def _key(device: str, nbox: int, nq: int) -> str:
     return f"{device}|boxes~2^{round(math.log2(max(nbox, 1)))}|windows~2^{round(math.log2(max(nq, 1)))}"
 
 
+def _time(fn, reps):
+    import torch
+    times = []
+    for r in range(reps + 1):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        if r:  # the first run warms the pool and caches
+            times.append(e0.elapsed_time(e1))
+    return statistics.median(times)
+
+
 def autotune(d_boxes: BBox, d_windows: BBox, fanouts=(8, 16, 32), warps=(8, 16, 32),
-             stage=(1, 0), chunks=(4096,), reps: int = 3, cache_path: str | None = DEFAULT_CACHE,
-             use_cache: bool = True) -> dict:
-    """Returns {"fanout", "warps_per_cta", "stage_levels", "chunk", "ms", "table"}."""
+             stage=(0, 1, 2, 3, 4), window_warps=(1, 2, 4), chunks=(1024, 4096, 16384),
+             reps: int = 3, cache_path: str | None = DEFAULT_CACHE, use_cache: bool = True) -> dict:
+    """Returns {"fanout", "warps_per_cta", "stage_levels", "warps_per_window",
+    "chunk", "ms", "table"}.  The search goes one dimension at a time, each
+    from the best so far: fanout x warps per CTA (every pair), then the
+    staging depth in whole levels, then the warps sharing a window, then the
+    output chunk; the table lists every configuration timed."""
     import torch
 
     device = torch.cuda.get_device_name()
@@ -43,35 +64,43 @@ def autotune(d_boxes: BBox, d_windows: BBox, fanouts=(8, 16, 32), warps=(8, 16, 
             return dict(cached, cached=True)
 
     table = []
+    trees = {}
+
+    def run(f, opts):
+        if f not in trees:
+            for old in list(trees):  # one candidate tree on the device at a time
+                del trees[old]
+            torch.cuda.empty_cache()
+            sorted_boxes, rt = build_into(d_boxes, f)
+            pairs = query_stats(rt, sorted_boxes, d_windows)["hits"]
+            cap = max(query_capacity(pairs), query_capacity(pairs) + 64 * 16384 * 148)
+            trees[f] = (sorted_boxes, rt, torch.empty(max(cap, 1), dtype=torch.int32, device="cuda"),
+                        torch.empty(max(cap, 1), dtype=torch.int32, device="cuda"),
+                        new_result_block())
+        sb, rt, fid, tid, res = trees[f]
+        ms = _time(lambda: query_into(rt, sb, d_windows, fid, tid, res, **opts), reps)
+        row = {"fanout": f, **opts, "ms": ms}
+        table.append(row)
+        return row
+
+    base = {"warps_per_cta": warps[0], "stage_levels": 2, "warps_per_window": 1, "chunk": 4096}
     best = None
     for f in fanouts:
-        sorted_boxes, rt = build_into(d_boxes, f)
-        pairs = query_stats(rt, sorted_boxes, d_windows)["hits"]
-        cap = query_capacity(pairs)
-        fid = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
-        tid = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
-        res = new_result_block()
         for w in warps:
-            for st in stage:
-                for ch in chunks:
-                    opts = {"warps_per_cta": w, "stage_levels": st, "chunk": ch}
-                    times = []
-                    for r in range(reps + 1):
-                        e0 = torch.cuda.Event(enable_timing=True)
-                        e1 = torch.cuda.Event(enable_timing=True)
-                        e0.record()
-                        query_into(rt, sorted_boxes, d_windows, fid[:cap], tid[:cap], res, **opts)
-                        e1.record()
-                        e1.synchronize()
-                        if r:  # the first run warms the pool and caches
-                            times.append(e0.elapsed_time(e1))
-                    ms = statistics.median(times)
-                    row = {"fanout": f, **opts, "ms": ms}
-                    table.append(row)
-                    if best is None or ms < best["ms"]:
-                        best = dict(row)
-        del fid, tid, sorted_boxes, rt
-        torch.cuda.empty_cache()
+            row = run(f, dict(base, warps_per_cta=w))
+            if best is None or row["ms"] < best["ms"]:
+                best = dict(row)
+    for dim, values in (("stage_levels", stage), ("warps_per_window", window_warps),
+                        ("chunk", chunks)):
+        cur = {k: best[k] for k in base}
+        for v in values:
+            if v == cur[dim]:
+                continue
+            row = run(best["fanout"], dict(cur, **{dim: v}))
+            if row["ms"] < best["ms"]:
+                best = dict(row)
+    trees.clear()
+    torch.cuda.empty_cache()
     best["table"] = table
     best["key"] = key
     if cache_path:
@@ -92,7 +121,7 @@ def autotune(d_boxes: BBox, d_windows: BBox, fanouts=(8, 16, 32), warps=(8, 16, 
 def query_opts(best: dict) -> dict:
     """The winner as keyword options for query/query_into/Plan."""
     return {"warps_per_cta": best["warps_per_cta"], "stage_levels": best["stage_levels"],
-            "chunk": best["chunk"]}
+            "warps_per_window": best.get("warps_per_window", 1), "chunk": best["chunk"]}
 
 
 __all__ = ["autotune", "query_opts", "DEFAULT_CACHE", "_lib"]

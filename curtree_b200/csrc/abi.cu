@@ -309,7 +309,8 @@ void crt_query_opts_default(crt_query_opts* o)
   std::memset(o, 0, sizeof(*o));
   o->mode = CRT_QUERY_PERSISTENT;
   o->sort_windows = 1;
-  o->stage_levels = 1;
+  o->stage_levels = 2;
+  o->warps_per_window = 1;
 }
 
 int64_t crt_query_capacity(int64_t pairs, const crt_query_opts* opts)

@@ -152,10 +152,11 @@ constexpr size_t kJobQueueBytes = offsetof(JobQueue, entries) + sizeof(RangeJob)
 __device__ __forceinline__ void fence_sc_gpu() { asm volatile("fence.sc.gpu;" ::: "memory"); }
 
 // Waits (lane 0) until queue index h is published, and takes the piece; 0 when
-// h will never be published (every window is done and h was not reserved) or
-// the bounded wait ran out (an error is recorded).
+// h will never be published (every ticket is taken, no warp still works on
+// one, and h was not reserved) or the bounded wait ran out (an error is
+// recorded).  ntickets: the ticket count of the launch.
 __device__ __forceinline__ int wait_piece(JobQueue* Q, const QueryCounters* ctr,
-                                          unsigned long long nq, long long h, RangeJob& out,
+                                          unsigned long long ntickets, long long h, RangeJob& out,
                                           int* err)
 {
   RangeJob* J = Q->entries + h;
@@ -175,7 +176,7 @@ __device__ __forceinline__ int wait_piece(JobQueue* Q, const QueryCounters* ctr,
       const unsigned long long t = ld_relaxed_ull(&ctr->ticket);
       fence_sc_gpu();
       const unsigned long long a = ld_relaxed_ull(&Q->active);
-      if (t >= nq && a == 0) {
+      if (t >= ntickets && a == 0) {
         fence_sc_gpu();
         if (ld_relaxed_ull(&Q->tail) <= (unsigned long long)h) return 0;
       }
@@ -419,6 +420,7 @@ struct PersistParams {
   int K;
   int stack_cap;
   int stage_n;  // nodes staged in shared memory (multiple of 4), 0 = none
+  int parts;    // warps sharing one window (shares of the root's children)
   int chunk;
   int32_t* fid;
   int32_t* tid;
@@ -517,6 +519,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     order = na == 0 ? nullptr : ((na & 1) ? P.order1 : P.order0);
   }
   const long long nq = (long long)P.ctr->nq;
+  const int parts = P.parts;
+  const long long ntickets = nq * parts;  // one ticket per (window, share)
   ChunkEmit emit;
   emit.fid = P.fid;
   emit.tid = P.tid;
@@ -537,12 +541,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
     unsigned long long t = 0;
     if (lane_id() == 0) t = atomicAdd(&P.ctr->ticket, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
-    if ((long long)t >= nq) break;
-    int q = order ? (int)order[t] : (int)t;
-    if (q < 0 || (long long)q >= nq) q = (int)t;  // only after a sort error (reported)
+    if ((long long)t >= ntickets) break;
+    const long long qi = parts == 1 ? (long long)t : (long long)t / parts;
+    const int part = parts == 1 ? 0 : (int)((long long)t - qi * parts);
+    int q = order ? (int)order[qi] : (int)qi;
+    if (q < 0 || (long long)q >= nq) q = (int)qi;  // only after a sort error (reported)
     emit.begin(q);
     traverse(P.T, C, P.K, lg, lc, P.W.xmin[q], P.W.ymin[q], P.W.xmax[q], P.W.ymax[q], stack,
-             P.stack_cap, emit, &P.ctr->error);
+             P.stack_cap, emit, &P.ctr->error, part, parts);
   }
   if (Q) {
     __syncwarp();
@@ -560,7 +566,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
       if (h >= kJobs) break;  // past the queue: never published
       RangeJob J{};
       int got = 0;
-      if (lane_id() == 0) got = wait_piece(Q, P.ctr, (unsigned long long)nq, h, J, &P.ctr->error);
+      if (lane_id() == 0) got = wait_piece(Q, P.ctr, (unsigned long long)ntickets, h, J, &P.ctr->error);
       if (!__shfl_sync(0xffffffffu, got, 0)) break;
       const long long first = __shfl_sync(0xffffffffu, J.first, 0);
       const long long slot = __shfl_sync(0xffffffffu, J.slot, 0);
@@ -853,7 +859,6 @@ static TraversalShape traversal_shape(int64_t nbox, int fanout)
 }
 
 constexpr int kDefaultChunk = 4096;
-constexpr int kStageMaxNodes = 2048;
 
 // Persistent traversal variants: CTA width and CTAs per SM, which fix the
 // register budget (65536 / (threads x CTAs)).  Wider CTAs share one staged
@@ -993,7 +998,7 @@ struct TraverseLaunch {
 static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
                                     const PersistScratch& S, bool sort, int stage_n,
                                     int32_t* fid, int32_t* tid, long long cap, int chunk,
-                                    int warps_per_cta)
+                                    int warps_per_cta, int parts)
 {
   const TraversalShape sh = traversal_shape(T.nbox, T.fanout);
   const PersistShape ps = persist_shape(sh.stack_cap, stage_n, warps_per_cta);
@@ -1007,6 +1012,7 @@ static TraverseLaunch make_traverse(const TreeView& T, const WindowView& W,
   P.K = sh.K;
   P.stack_cap = sh.stack_cap;
   P.stage_n = ps.stage_n;
+  P.parts = parts;
   P.chunk = chunk;
   P.fid = fid;
   P.tid = tid;
@@ -1043,21 +1049,47 @@ static void enqueue_post(const PersistScratch& S, int32_t* fid, int32_t* tid, lo
   CRT_LAUNCHED(3);
 }
 
-static int stage_nodes_for(const crt_rtree_f32& rt, bool want)
+// Nodes of the root and the `levels` whole tree levels below it, rounded up
+// to a multiple of 4 (16-byte bulk copies; the extra nodes are staged too)
+// and at most R_sz rounded down to one; 0 when staging is off or the node
+// arrays are not 16-byte aligned.
+static int stage_nodes_for(const crt_rtree_f32& rt, int64_t nbox, int levels)
 {
-  if (!want || rt.sz <= 0) return 0;
+  if (levels <= 0 || rt.sz <= 0) return 0;
   const void* arrs[6] = {rt.xmin, rt.ymin, rt.xmax, rt.ymax, rt.pos, rt.len};
   for (auto p : arrs)
     if (((uintptr_t)p & 15u) != 0) return 0;
-  int n = std::min(rt.sz, kStageMaxNodes);
-  // whole levels only, counted from the root: nodes [0, n)
-  return n & ~3;
+  std::vector<int64_t> lv;  // leaf-parent level first, root last
+  const int L = tree_levels(std::max<int64_t>(nbox, 1), std::max(rt.fanout, 2), lv);
+  int64_t n = 0;
+  for (int i = 0; i <= levels && i < L; i++) n += lv[L - 1 - i];
+  n = std::min<int64_t>((int64_t)rt.sz & ~(int64_t)3, (n + 3) & ~(int64_t)3);
+  return (int)n;
+}
+
+// The deepest staging (at most `levels` levels) whose nodes fit beside the
+// warps' stacks at the variant's full occupancy.
+static int fit_stage_nodes(const crt_rtree_f32& rt, int64_t nbox, int levels, int stack_cap,
+                           int warps_per_cta)
+{
+  for (int k = levels; k > 0; k--) {
+    const int sn = stage_nodes_for(rt, nbox, k);
+    if (sn > 0 && persist_shape(stack_cap, sn, warps_per_cta).stage_n == sn) return sn;
+  }
+  return 0;
 }
 
 static long long max_holes_for(int stack_cap, int stage_n, int warps_per_cta)
 {
   const PersistShape ps = persist_shape(stack_cap, stage_n, warps_per_cta);
   return (long long)persistent_grid(*ps.v, ps.smem) * (ps.v->threads / 32);
+}
+
+// Warps per window of the persistent form (0 = 1); -1 for an unsupported value.
+static int window_parts(const crt_query_opts& o)
+{
+  const int w = o.warps_per_window <= 0 ? 1 : o.warps_per_window;
+  return (w == 1 || w == 2 || w == 4) ? w : -1;
 }
 
 int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox_f32& qbox,
@@ -1128,8 +1160,11 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
 
   // persistent
   const bool sort = opts.sort_windows != 0 && nq > 1;
-  const int stage_n = stage_nodes_for(rt, opts.stage_levels != 0);
+  const int stage_n = fit_stage_nodes(rt, rbox.sz, opts.stage_levels, sh.stack_cap,
+                                      opts.warps_per_cta);
   const int chunk = opts.chunk >= 64 ? opts.chunk : kDefaultChunk;
+  const int parts = window_parts(opts);
+  if (parts < 0) return fail(CRT_ERR_INVALID_ARG, "query: warps_per_window must be 1, 2 or 4");
   if (!persist_shape(sh.stack_cap, stage_n, opts.warps_per_cta).v)
     return fail(CRT_ERR_NOT_SUPPORTED, "query: traversal stack too large");
   const long long max_holes = max_holes_for(sh.stack_cap, stage_n, opts.warps_per_cta);
@@ -1146,7 +1181,7 @@ int query_into(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbox
   CRT_LAUNCHED(1);
   enqueue_pre(W, nq, S, sort, stream);
   cudaError_t e = launch_traverse(make_traverse(T, W, S, sort, stage_n, fid, tid, capacity, chunk,
-                                                opts.warps_per_cta),
+                                                opts.warps_per_cta, parts),
                                   stream);
   enqueue_post(S, fid, tid, capacity, d_result, stream);
   cudaFreeAsync(scr, stream);
@@ -1363,13 +1398,18 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   p->W = WindowView{qbox.xmin, qbox.ymin, qbox.xmax, qbox.ymax, max_nq};
   p->max_nq = max_nq;
   p->sort = opts.sort_windows != 0 && max_nq > 1;
-  p->stage_n = stage_nodes_for(rt, opts.stage_levels != 0);
   p->chunk = opts.chunk >= 64 ? opts.chunk : kDefaultChunk;
+  const int parts = window_parts(opts);
+  if (parts < 0) {
+    delete p;
+    return fail(CRT_ERR_INVALID_ARG, "plan: warps_per_window must be 1, 2 or 4");
+  }
   p->fid = fid;
   p->tid = tid;
   p->cap = capacity;
   p->res = res;
   const TraversalShape sh = traversal_shape(rbox.sz, rt.fanout);
+  p->stage_n = fit_stage_nodes(rt, rbox.sz, opts.stage_levels, sh.stack_cap, opts.warps_per_cta);
   if (!persist_shape(sh.stack_cap, p->stage_n, opts.warps_per_cta).v) {
     delete p;
     return fail(CRT_ERR_NOT_SUPPORTED, "plan: traversal stack too large");
@@ -1387,7 +1427,7 @@ int plan_create(const crt_rtree_f32& rt, const crt_bbox_f32& rbox, const crt_bbo
   set_nq_kernel<<<1, 1, 0, stream>>>(p->S.ctr, max_nq);
   CRT_LAUNCHED(1);
   p->traverse = make_traverse(p->T, p->W, p->S, p->sort, p->stage_n, fid, tid, capacity, p->chunk,
-                              opts.warps_per_cta);
+                              opts.warps_per_cta, parts);
   // capture the whole query on a private stream; a window-sorting plan
   // orders exactly max_nq windows, so it only runs with nq == max_nq
   // (plan_set_nq enforces it); without sorting the kernel reads the live

@@ -190,16 +190,20 @@ __device__ __forceinline__ void copy_range(const int* __restrict__ bid, long lon
   if (lane < count - done) put_pair(fid, tid, slot0 + done + lane, cap, __ldg(src + done + lane), q);
 }
 
+// part / nparts: this warp takes the part-th of nparts equal shares of the
+// root's children (several warps sharing one window); the shares' subtrees
+// are disjoint, so their hits together are the window's.
 template <class Emit, bool kContain = true>
 __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, int K,
                                          int lane_g, int lane_c, float x1, float y1, float x2,
                                          float y2, FrontierEntry* stack, int stack_cap,
-                                         Emit& emit, int* err)
+                                         Emit& emit, int* err, int part = 0, int nparts = 1)
 {
   const int lane = (int)lane_id();
   const uint32_t lt = lanemask_lt();
   const int f = T.fanout;
   if (T.rsz == 0) {
+    if (part != 0) return;
     // one-box (or empty) tree: no nodes, test the boxes directly
     for (int base = 0; base < T.nbox; base += 32) {
       int s = base + lane;
@@ -219,6 +223,12 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
   {
     int rp, rl;
     load_node_link(T, C, 0, rp, rl);
+    if (nparts > 1) {
+      const int a = (int)((long long)rl * part / nparts);
+      const int b = (int)((long long)rl * (part + 1) / nparts);
+      rp += a;
+      rl = b - a;
+    }
     if (contain) rl |= max(T.nlev - 2, 0) << kLenBits;
     if (lane == 0) stack[0] = make_int2(rp, rl);
   }

@@ -253,8 +253,10 @@ class PairDigest:
         return c, h, int(self.bad.item())
 
 
-def query_capacity(pairs: int, mode: int = _lib.CRT_QUERY_PERSISTENT) -> int:
-    o = _lib.default_opts(mode=mode)
+def query_capacity(pairs: int, mode: int = _lib.CRT_QUERY_PERSISTENT, **opts) -> int:
+    """Output slots for `pairs` pairs in this mode (persistent: plus the
+    per-warp chunk slack of the options' chunk)."""
+    o = _lib.default_opts(mode=mode, **opts)
     return int(load().crt_query_capacity(pairs, ctypes.byref(o)))
 
 
@@ -293,7 +295,9 @@ def query(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, mode: int = _lib.CRT_QUERY_PE
     """Synchronous extended query with overflow-and-retry; returns
     (fid, tid) torch tensors of exactly `count` pairs (and offsets in plain mode)."""
     res = new_result_block()
-    cap = capacity if capacity is not None else query_capacity(max(64 * d_qbox.sz, 1024), mode)
+    chunk = {"chunk": opts["chunk"]} if "chunk" in opts else {}
+    cap = capacity if capacity is not None else query_capacity(max(64 * d_qbox.sz, 1024), mode,
+                                                               **chunk)
     nq = d_qbox.sz
     for _ in range(3):
         fid = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
@@ -307,7 +311,7 @@ def query(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, mode: int = _lib.CRT_QUERY_PE
         if not r["overflow"]:
             n = r["count"]
             return (fid[:n], tid[:n], offs) if offs is not None else (fid[:n], tid[:n])
-        cap = query_capacity(r["required"], mode)
+        cap = query_capacity(r["required"], mode, **chunk)
     raise _lib.CrtError(_lib.CRT_ERR_OUTPUT_OVERFLOW, "query")
 
 

@@ -146,13 +146,17 @@ enum {
 };
 
 typedef struct {
-  int mode;          /* CRT_QUERY_PERSISTENT or CRT_QUERY_PLAIN */
-  int sort_windows;  /* persistent: visit windows in Morton order of their centres (default 1) */
-  int stage_levels;  /* persistent: stage the top tree levels in shared memory (default 1) */
-  int warps_per_cta; /* persistent: 8, 16 or 32 warps per CTA (0 = default) */
-  int chunk;         /* persistent: output slots a warp reserves at a time (0 = default) */
-  int no_contain;    /* 1: test every box even under nodes the window contains */
-  int reserved[2];
+  int mode;             /* CRT_QUERY_PERSISTENT or CRT_QUERY_PLAIN */
+  int sort_windows;     /* persistent: visit windows in Morton order of their centres (default 1) */
+  int stage_levels;     /* persistent: whole tree levels below the root staged in shared memory
+                           with bulk async copies (default 2, 0 = none; levels that do not fit
+                           beside the warps' frontier stacks are left out) */
+  int warps_per_cta;    /* persistent: 8, 16 or 32 warps per CTA (0 = default) */
+  int chunk;            /* persistent: output slots a warp reserves at a time (0 = default) */
+  int no_contain;       /* 1: test every box even under nodes the window contains */
+  int warps_per_window; /* persistent: warps sharing one window, each taking an equal share of
+                           the root's children (1, 2 or 4; 0 = 1) */
+  int reserved[1];
 } crt_query_opts;
 
 void crt_query_opts_default(crt_query_opts* o);

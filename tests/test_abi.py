@@ -77,4 +77,4 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
 
 def test_opts_defaults():
     o = _lib.default_opts()
-    assert o.mode == _lib.CRT_QUERY_PERSISTENT and o.sort_windows == 1 and o.stage_levels == 1
+    assert o.mode == _lib.CRT_QUERY_PERSISTENT and o.sort_windows == 1 and o.stage_levels == 2 and o.warps_per_window == 1

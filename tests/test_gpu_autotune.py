@@ -23,10 +23,13 @@ def test_autotune_picks_and_caches():
     dq = C.BBox.from_host(q)
     with tempfile.TemporaryDirectory() as tmp:
         cache = os.path.join(tmp, "tune.json")
-        best = autotune(d, dq, fanouts=(8, 16, 32), warps=(8, 32), stage=(1, 0), reps=2,
-                        cache_path=cache)
+        best = autotune(d, dq, fanouts=(8, 16, 32), warps=(8, 32), stage=(0, 2, 3),
+                        window_warps=(1, 2), chunks=(1024, 4096), reps=2, cache_path=cache)
         assert best["fanout"] in (8, 16, 32) and best["warps_per_cta"] in (8, 32)
-        assert len(best["table"]) == 3 * 2 * 2
+        # every fanout x warps pair, then each other dimension's other values
+        assert len(best["table"]) == 3 * 2 + 2 + 1 + 1
+        assert {r["stage_levels"] for r in best["table"]} == {0, 2, 3}
+        assert {r["warps_per_window"] for r in best["table"]} == {1, 2}
         assert best["ms"] == min(r["ms"] for r in best["table"])
         again = autotune(d, dq, cache_path=cache)
         assert again.get("cached") and again["fanout"] == best["fanout"]

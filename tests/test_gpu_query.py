@@ -52,6 +52,10 @@ def all_forms(crt, d, rt, dq):
     out["persistent_unsorted"] = canon(*crt.query(rt, d, dq, sort_windows=0))
     out["persistent_unstaged"] = canon(*crt.query(rt, d, dq, stage_levels=0))
     out["persistent_small_chunk"] = canon(*crt.query(rt, d, dq, chunk=64))
+    out["persistent_2_warps_per_window"] = canon(*crt.query(rt, d, dq, warps_per_window=2))
+    out["persistent_4_warps_per_window"] = canon(*crt.query(rt, d, dq, warps_per_window=4,
+                                                           warps_per_cta=32))
+    out["persistent_staged_4_levels"] = canon(*crt.query(rt, d, dq, stage_levels=4))
     return out
 
 
@@ -404,3 +408,27 @@ def test_pairs_digest_of_a_query_equals_oracle_stats(crt):
     gc, gh, bad = dg.to_host()
     assert bad == 0 and want.total > 100_000
     assert np.array_equal(gc, want.counts) and np.array_equal(gh, want.hashes)
+
+
+def test_bad_warps_per_window_is_rejected(crt):
+    import torch
+    b = D.uniform_boxes(5000, seed=44)
+    q = D.uniform_windows(100, seed=144)
+    d, rt, dq, want = setup(crt, b, q, 10)
+    fid = torch.empty(1 << 16, dtype=torch.int32, device="cuda")
+    tid = torch.empty(1 << 16, dtype=torch.int32, device="cuda")
+    res = crt.new_result_block()
+    with pytest.raises(crt.CrtError):
+        crt.query_into(rt, d, dq, fid, tid, res, warps_per_window=3)
+
+
+@pytest.mark.parametrize("levels", [0, 1, 2, 3, 4, 9])
+def test_staging_depths_are_exact(crt, levels):
+    """Whole levels staged (as many of `levels` as fit) give the oracle's pairs,
+    with windows shared by 1 or 2 warps."""
+    b = D.clustered_boxes(400_000, seed=45)
+    q = D.mixed_windows(3000, b, seed=145, lo=1e-5, hi=5e-2)
+    d, rt, dq, want = setup(crt, b, q, 8)
+    for wpw in (1, 2):
+        got = canon(*crt.query(rt, d, dq, stage_levels=levels, warps_per_window=wpw))
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), (levels, wpw)
