@@ -332,7 +332,7 @@ def query_stream(d_rt: RTree, d_rbox: BBox, d_qbox: BBox, consume, capacity: int
     cap = int(capacity)
     # pairs a batch may need and still fit: the persistent form reserves
     # output in per-warp chunks, which may leave one partly used chunk each
-    usable = cap - query_capacity(0, mode)
+    usable = cap - query_capacity(0, mode, **({"chunk": opts["chunk"]} if "chunk" in opts else {}))
     if usable <= 0:
         raise _lib.CrtError(_lib.CRT_ERR_INVALID_ARG,
                             f"query_stream: capacity {cap} is below the form's slack")
