@@ -474,8 +474,8 @@ __global__ void __launch_bounds__(kSortThreads, 2)
 #pragma unroll
   for (int i = 0; i < kSortIpt; i++) {
     const int j = wbase + 32 * i;
-    if (j < tile_n) {
-      const int pos = (int)(wh[(key[i] >> shift) & kMask] + rank[i]);
+    const int pos = (int)(wh[(key[i] >> shift) & kMask] + rank[i]);
+    if (j < tile_n && (unsigned)pos < (unsigned)kSortTile) {  // pos < tile_n by construction
       s_key[pos] = key[i];
       if (first) {
         s_val[pos] = (uint32_t)(base + j);
