@@ -17,12 +17,14 @@ struct SortBufs {
 };
 
 // Radix digits of the 32-bit sort keys: kDigits digits of kDigitBits bits
-// from the least significant end, the last one narrower (10 + 10 + 10 + 2:
-// keys whose top two bits never vary -- every Morton key of coordinates in
-// [0, 2^15) -- sort in three passes).  Histograms and bucket starts keep
-// kBins entries per digit.
+// from the least significant end, the last one narrower when kDigitBits does
+// not divide 32.  Histograms and bucket starts keep kBins entries per digit.
+// 8-bit digits (four passes, uniform digits skipped) measured faster on a
+// B200 than 10 + 10 + 10 + 2 (three passes for 30-bit Morton keys): 2.74
+// against 3.43 ms for 100M keys, the 1024-bin passes paying more for ranking,
+// bin scans and look-back than the fourth pass costs.
 #ifndef CRT_SORT_DIGIT_BITS
-#define CRT_SORT_DIGIT_BITS 10
+#define CRT_SORT_DIGIT_BITS 8
 #endif
 constexpr int kDigitBits = CRT_SORT_DIGIT_BITS;
 constexpr int kBins = 1 << kDigitBits;

@@ -1480,10 +1480,20 @@ int plan_launch(void* hp, cudaStream_t stream)
   NvtxRange range("crt_plan_launch");
   Plan* p = (Plan*)hp;
   cudaEvent_t a = p->own[0], b = p->own[1];
-  prof_register("traverse_persistent", &a, &b);  // leaves the plan's own pair when off
-  cudaError_t e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[0], a);
-  if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[1], b);
-  if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, stream);
+  cudaError_t e = cudaSuccess;
+  if (prof_register("traverse_persistent", &a, &b)) {
+    // this launch records a fresh pair (read and destroyed when the timings
+    // are collected); the nodes go back to the plan's own events right after,
+    // so the instantiated graph never refers to a destroyed event
+    e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[0], a);
+    if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[1], b);
+    if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, stream);
+    cudaError_t r = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[0], p->own[0]);
+    if (r == cudaSuccess) r = cudaGraphExecEventRecordNodeSetEvent(p->exec, p->ev_node[1], p->own[1]);
+    if (e == cudaSuccess) e = r;
+  } else {
+    e = cudaGraphLaunch(p->exec, stream);
+  }
   if (e != cudaSuccess) return cuda_fail(e, "plan_launch");
   // window keys, sort plan, four sort passes; the traversal; hole sort,
   // prefix and compaction
