@@ -360,6 +360,13 @@ def run_ours(args, rank, world, dist):
     hbm_peak, peak_kind = peaks()
     out = {}
 
+    # ---- the reference's own small case through the drop-in calls, first:
+    # measured like the reference's run of it, on a device whose memory pools
+    # the large legs have not filled yet
+    if "config1" not in skip and rank == 0:
+        out["config1"] = config1_leg(args, C, stream)
+        torch.cuda.empty_cache()
+
     # ---- inputs resident in HBM -------------------------------------------
     boxes, windows = make_query_inputs(rank, args.boxes, args.windows)
     d_in = C.BBox.from_host(boxes)
@@ -525,11 +532,6 @@ def run_ours(args, rank, world, dist):
     # ---- ingest: MBR text file -> device boxes ---------------------------------
     if "ingest" not in skip and rank == 0:
         out["ingest"] = ingest_leg(args, C, L, stream)
-        torch.cuda.empty_cache()
-
-    # ---- the reference's own small case through the drop-in calls -----------------
-    if "config1" not in skip and rank == 0:
-        out["config1"] = config1_leg(args, C, stream)
         torch.cuda.empty_cache()
 
     # ---- bulk load ------------------------------------------------------------

@@ -615,138 +615,6 @@ __global__ void __launch_bounds__(kLevelThreads)
 }
 
 // ---------------------------------------------------------------------------
-// 4. leaf level through shared memory
-// ---------------------------------------------------------------------------
-// The leaf-parent level for fanout <= kLeafChunk.  Each CTA takes the
-// parents whose children fill at most kChunk sorted slots:
-//   1. the record slots of those children (coalesced 4-byte loads),
-//   2. two 16-byte async copies per record from the AoS copy into shared
-//      memory (cp.async: the gathers are in flight without holding
-//      registers, so many CTAs per SM keep many gathers in flight),
-//   3. per warp, lanes mapped to (parent, child) as in the traversal: each
-//      lane writes its child's permuted box (nearly contiguous stores) and
-//      the parent's MBR is a segmented min/max over the group's lanes with
-//      shuffles (fminf/fmaxf, reduce_op's device min/max; no neutral
-//      element, so an all-NaN group stays NaN as in the reference).
-constexpr int kLeafThreads = 256;
-constexpr int kLeafWarps = kLeafThreads / 32;
-constexpr int kLeafChunk = 1024;
-
-template <int kChunk>
-__global__ void __launch_bounds__(kLeafThreads, (227 * 1024) / (kChunk * 32 + 1024))
-    leaf_gather_kernel(int fanout, int parents_per_cta, int64_t n, int64_t nparent,
-                       int64_t parent_start, int64_t pos_base, const uint32_t* __restrict__ vals0,
-                       const uint32_t* __restrict__ vals1, const BuildCtrl* __restrict__ ctrl,
-                       const Box32* __restrict__ aos, float* __restrict__ oxmin,
-                       float* __restrict__ oymin, float* __restrict__ oxmax,
-                       float* __restrict__ oymax, int* __restrict__ oid,
-                       float* __restrict__ nxmin, float* __restrict__ nymin,
-                       float* __restrict__ nxmax, float* __restrict__ nymax,
-                       int* __restrict__ npos, int* __restrict__ nlen)
-{
-  extern __shared__ __align__(32) unsigned char leaf_smem[];
-  Box32* s_rec = (Box32*)leaf_smem;
-  const int64_t p0 = (int64_t)blockIdx.x * parents_per_cta;
-  const int64_t p1 = min(nparent, p0 + parents_per_cta);
-  if (p0 >= p1) return;
-  const int f = fanout;
-  const int64_t c0 = p0 * f;
-  const int m = (int)(min(n, p1 * f) - c0);  // <= parents_per_cta * f <= kChunk
-  const uint32_t* __restrict__ sorted = (ctrl->n_active & 1) ? vals1 : vals0;
-
-  constexpr int kPer = kChunk / kLeafThreads;
-  uint32_t src[kPer];
-#pragma unroll
-  for (int u = 0; u < kPer; u++) {
-    const int i = threadIdx.x + u * kLeafThreads;
-    uint32_t v = i < m ? __ldg(sorted + c0 + i) : 0u;
-    if ((int64_t)v >= n) v = i < m ? (uint32_t)(c0 + i) : 0u;  // only after a sort error (reported)
-    src[u] = v;
-  }
-#pragma unroll
-  for (int u = 0; u < kPer; u++) {
-    const int i = threadIdx.x + u * kLeafThreads;
-    if (i < m) {
-      const uint32_t d = smem_u32(s_rec + i);
-      const char* g = (const char*)(aos + src[u]);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16u), "l"(g + 16)
-                   : "memory");
-    }
-  }
-  asm volatile("cp.async.commit_group;" ::: "memory");
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  __syncthreads();
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int K, g, c;
-  if (f <= 32) {
-    K = 32 / f;
-    g = lane / f;
-    c = lane - g * f;
-    if (g >= K) g = -1;  // spare lanes
-  } else {
-    K = 1;
-    g = 0;
-    c = lane;
-  }
-  const int nchunks = f <= 32 ? 1 : (f + 31) / 32;
-  for (int64_t pb = p0 + (int64_t)warp * K; pb < p1; pb += (int64_t)kLeafWarps * K) {
-    const int64_t p = pb + (g < 0 ? 0 : g);
-    const bool have = g >= 0 && p < p1;
-    const int64_t first = p * f;  // the parent's first child slot
-    const int glen = have ? (int)min((int64_t)f, n - first) : 0;
-    float a = 0.f, b = 0.f, cc = 0.f, d = 0.f;
-    for (int ch = 0; ch < nchunks; ch++) {
-      const int k = ch * 32 + c;  // child index within the parent
-      const int clen = glen - ch * 32;  // children of this parent from this chunk on
-      const bool valid = have && k < glen;
-      float x0 = 0.f, y0 = 0.f, x1 = 0.f, y1 = 0.f;
-      if (valid) {
-        const Box32 r = s_rec[(int)(first + k - c0)];
-        x0 = r.mbr.x;
-        y0 = r.mbr.y;
-        x1 = r.mbr.z;
-        y1 = r.mbr.w;
-        const int64_t s = first + k;
-        __stcs(oxmin + s, x0);
-        __stcs(oymin + s, y0);
-        __stcs(oxmax + s, x1);
-        __stcs(oymax + s, y1);
-        __stcs(oid + s, r.idp.x);
-      }
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const float u0 = __shfl_down_sync(0xffffffffu, x0, off);
-        const float u1 = __shfl_down_sync(0xffffffffu, y0, off);
-        const float u2 = __shfl_down_sync(0xffffffffu, x1, off);
-        const float u3 = __shfl_down_sync(0xffffffffu, y1, off);
-        if (valid && c + off < clen) {
-          x0 = fminf(x0, u0);
-          y0 = fminf(y0, u1);
-          x1 = fmaxf(x1, u2);
-          y1 = fmaxf(y1, u3);
-        }
-      }
-      if (ch == 0) {
-        a = x0; b = y0; cc = x1; d = y1;
-      } else if (clen > 0) {
-        a = fminf(a, x0); b = fminf(b, y0); cc = fmaxf(cc, x1); d = fmaxf(d, y1);
-      }
-    }
-    if (have && c == 0) {
-      const int64_t o = parent_start + p;
-      nxmin[o] = a;
-      nymin[o] = b;
-      nxmax[o] = cc;
-      nymax[o] = d;
-      npos[o] = (int)(pos_base + first);
-      nlen[o] = glen;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 int tree_levels(int64_t n, int fanout, std::vector<int64_t>& lv)
@@ -883,17 +751,7 @@ int build_tree(const float* in_xmin, const float* in_ymin, const float* in_xmax,
       int npc = (int)std::max<int64_t>(1, std::min<int64_t>(kLevelThreads, kLevelChunk / fanout));
       unsigned g = (unsigned)cdiv(np, npc);
       ProfScope ps("level", stream);
-      if (l == 0 && fanout <= kLeafChunk) {
-        const int ppc = kLeafChunk / fanout;
-        const size_t smem = (size_t)kLeafChunk * sizeof(Box32);
-        // the most shared memory per SM, so that six CTAs fit
-        cudaFuncSetAttribute(leaf_gather_kernel<kLeafChunk>,
-                             cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        leaf_gather_kernel<kLeafChunk><<<(unsigned)cdiv(np, ppc), kLeafThreads, smem, stream>>>(
-            fanout, ppc, n, np, parent_start, rsz, bufs.vals[0], bufs.vals[1], ctrl, aos, out_xmin,
-            out_ymin, out_xmax, out_ymax, out_id, nxmin, nymin, nxmax, nymax, npos, nlen);
-      } else if (l == 0)
+      if (l == 0)
         level_kernel<true><<<g, kLevelThreads, 0, stream>>>(
             npc, fanout, nchild, np, parent_start, rsz, bufs.vals[0], bufs.vals[1], ctrl, aos,
             out_xmin, out_ymin, out_xmax, out_ymax, out_id, nxmin, nymin, nxmax, nymax, npos,
