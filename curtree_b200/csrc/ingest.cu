@@ -63,7 +63,6 @@ constexpr int kScanThreads = 1024;
 constexpr int kParseThreads = 256;
 constexpr int kTextPad = 64;        // '\n' bytes after the last tile
 constexpr int kFieldMax = 62;       // longest field the fast path takes
-constexpr int64_t kFallbackCap = 1 << 20;
 constexpr int kStageThreads = 16;
 constexpr size_t kStageChunk = size_t(4) << 20;
 
@@ -683,7 +682,7 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
 
   int64_t first_bad = -1;
   if (m > 0) {
-    const int64_t cap = std::min(m, kFallbackCap);
+    const int64_t cap = m;  // room for every record: the host never reads the whole file for them
     int64_t* starts = S.get<int64_t>((size_t)m * 8);
     int64_t* fb = S.get<int64_t>((size_t)cap * 24);
     if (!starts || !fb) {
@@ -719,29 +718,50 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
       }
       const char* end = base + src.len;
       std::vector<FixRecord> fix;
-      bool whole = c > cap;  // too many for the list: the host loader reads the file
+      bool whole = false;
       if (!whole) {
         std::vector<int64_t> h_fb((size_t)c * 3);
         e = cudaMemcpy(h_fb.data(), fb, (size_t)c * 24, cudaMemcpyDeviceToHost);
-        for (int64_t j = 0; j < c && e == cudaSuccess && !whole; j++) {
-          const int64_t k = h_fb[3 * j], s0 = h_fb[3 * j + 1], next = h_fb[3 * j + 2];
-          float v[4];
-          int rid = 0;
-          const char* stop = parse_mbr_record(base + s0, end, v, rid);
-          if (!stop) {
-            if (first_bad < 0 || k < first_bad) first_bad = k;
-            continue;
+        // host threads parse the listed records, each into its own part
+        const int nt = (int)std::max<int64_t>(
+            1, std::min<int64_t>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())),
+                                 c / 4096 + 1));
+        std::vector<std::vector<FixRecord>> parts((size_t)nt);
+        std::vector<int64_t> bad((size_t)nt, -1);
+        std::vector<char> moved((size_t)nt, 0);
+        auto work = [&](int t) {
+          const int64_t j0 = c * t / nt, j1 = c * (t + 1) / nt;
+          for (int64_t j = j0; j < j1; j++) {
+            const int64_t k = h_fb[3 * j], s0 = h_fb[3 * j + 1], next = h_fb[3 * j + 2];
+            float v[4];
+            int rid = 0;
+            const char* stop = parse_mbr_record(base + s0, end, v, rid);
+            if (!stop) {
+              if (bad[t] < 0 || k < bad[t]) bad[t] = k;
+              continue;
+            }
+            // a record that does not end where the line scan put the next one
+            // (records across lines, several on a line): fscanf's records are
+            // not the lines here, so the host loader reads the whole file
+            if (next >= 0 ? stop != base + next : (m < n || n < 0) && stop != end) {
+              moved[t] = 1;
+              return;
+            }
+            FixRecord f{k, 0, 0, 0, 0, rid, 0};
+            mbr_box(v, r, &f.xmin, &f.ymin, &f.xmax, &f.ymax);
+            parts[t].push_back(f);
           }
-          // a record that does not end where the line scan put the next one
-          // (records across lines, several on a line): fscanf's records are
-          // not the lines here, so the host loader reads the whole file
-          if (next >= 0 ? stop != base + next : (m < n || n < 0) && stop != end) {
-            whole = true;
-            break;
-          }
-          FixRecord f{k, 0, 0, 0, 0, rid, 0};
-          mbr_box(v, r, &f.xmin, &f.ymin, &f.xmax, &f.ymax);
-          fix.push_back(f);
+        };
+        if (e == cudaSuccess) {
+          std::vector<std::thread> th;
+          for (int t = 1; t < nt; t++) th.emplace_back(work, t);
+          work(0);
+          for (auto& x : th) x.join();
+        }
+        for (int t = 0; t < nt; t++) {
+          whole = whole || moved[t];
+          if (bad[t] >= 0 && (first_bad < 0 || bad[t] < first_bad)) first_bad = bad[t];
+          fix.insert(fix.end(), parts[t].begin(), parts[t].end());
         }
       }
       if (whole && e == cudaSuccess) {
