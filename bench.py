@@ -400,9 +400,7 @@ def run_ours(args, rank, world, dist):
 
     # ---- persistent form (graph plan) -------------------------------------
     L.crt_profile_enable(1)
-    qopts = {"warps_per_cta": args.warps, "stage_levels": args.stage,
-             "sort_windows": args.sort_windows, "warps_per_window": args.window_warps,
-             "chunk": args.chunk}
+    qopts = persistent_opts(args)
     plan = C.Plan(rt, sorted_box, d_win, fid, tid, res, **qopts)
     for _ in range(args.warmup):
         plan.launch()
@@ -566,6 +564,14 @@ def parity_headline(args, boxes, windows, rt, sorted_box, digests, world):
             "seconds": time.perf_counter() - t0}
 
 
+def persistent_opts(args):
+    """The persistent form's options the headline runs with (the autotuner's
+    choice unless given)."""
+    return {"warps_per_cta": args.warps, "stage_levels": args.stage,
+            "sort_windows": args.sort_windows, "warps_per_window": args.window_warps,
+            "chunk": args.chunk}
+
+
 def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, dist, world):
     """End to end through the C ABI with host buffers, per step: the windows
     H2D from pinned host memory, the query, the result block D2H (the pair
@@ -674,7 +680,7 @@ def e2e_leg(args, C, L, rt, sorted_box, windows, pairs, fid, tid, res, stream, d
 
     def step_pairs():
         h2d_windows()
-        C.query_into(rt, sorted_box, d_win, fid, tid, res)
+        C.query_into(rt, sorted_box, d_win, fid, tid, res, **persistent_opts(args))
         n = count()
         h_fid[:n].copy_(fid[:n], non_blocking=True)
         h_tid[:n].copy_(tid[:n], non_blocking=True)
