@@ -63,6 +63,7 @@ constexpr int kScanThreads = 1024;
 constexpr int kParseThreads = 256;
 constexpr int kTextPad = 64;        // '\n' bytes after the last tile
 constexpr int kFieldMax = 62;       // longest field the fast path takes
+constexpr int64_t kFallbackList = 1 << 20;  // undecided records listed at first
 constexpr int kStageThreads = 16;
 constexpr size_t kStageChunk = size_t(4) << 20;
 
@@ -682,7 +683,7 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
 
   int64_t first_bad = -1;
   if (m > 0) {
-    const int64_t cap = m;  // room for every record: the host never reads the whole file for them
+    int64_t cap = std::min<int64_t>(m, kFallbackList);
     int64_t* starts = S.get<int64_t>((size_t)m * 8);
     int64_t* fb = S.get<int64_t>((size_t)cap * 24);
     if (!starts || !fb) {
@@ -710,6 +711,29 @@ int ingest(Source& src, int64_t n, float r, bool alloc, Outputs out, crt_bbox_f3
       return cuda_fail(e, "read_mbr_csv_device: parse");
     }
     const int64_t c = (int64_t)h_ctr[1];
+    if (c > cap) {
+      // more undecided records than the list holds: list them all (the
+      // parse runs again into a list of their exact count)
+      cap = c;
+      fb = S.get<int64_t>((size_t)cap * 24);
+      if (!fb) {
+        release();
+        return fail(CRT_ERR_OOM, "read_mbr_csv_device: device allocation failed");
+      }
+      e = cudaMemsetAsync(ctr + 1, 0, 8, stream);
+      if (e == cudaSuccess) {
+        mbr_parse_kernel<<<(unsigned)grid, kParseThreads, 0, stream>>>(
+            (const uint8_t*)d_text, starts, m, r, out.xmin, out.ymin, out.xmax, out.ymax, out.id,
+            ctr + 1, fb, cap);
+        CRT_LAUNCHED(1);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "read_mbr_csv_device: parse");
+      }
+    }
     if (c > 0) {
       const char* base = src.view();
       if (!base) {

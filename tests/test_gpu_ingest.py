@@ -292,8 +292,9 @@ def test_large_file_counts_and_prefixes(crt):
 
 
 def test_many_host_parsed_records(crt):
-    """More records than the device's list of host-parsed records holds: the
-    host loader parses the whole file, with the same result."""
+    """More undecided records (hex spellings) than the device's first list
+    holds: the parse runs again into a list of their exact count, host
+    threads finish them, and the result is the host loader's."""
     rng = np.random.default_rng(5)
     n = (1 << 20) + 5000
     xs = rng.uniform(-10, 10, (n, 4))
