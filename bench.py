@@ -366,6 +366,8 @@ def run_ours(args, rank, world, dist):
     if "config1" not in skip and rank == 0:
         out["config1"] = config1_leg(args, C, stream)
         torch.cuda.empty_cache()
+        out["small_windows"] = small_windows_leg(args, C, stream)
+        torch.cuda.empty_cache()
 
     # ---- inputs resident in HBM -------------------------------------------
     boxes, windows = make_query_inputs(rank, args.boxes, args.windows)
@@ -1118,6 +1120,63 @@ def ingest_leg(args, C, L, stream):
                         "crt_read_mbr_csv_device(path, n, r=0)"}
 
 
+def small_windows_case():
+    """A batch both GPU paths answer: 10M uniform boxes (side U[0,1e-3]) and
+    1M windows with side U[0,1e-3] (about 10 hits each), small enough for
+    the reference's bfs_frontier, whose 32-window blocks stop past 1024
+    frontier nodes (src/rtree_bfs_frontier.cuh:46-48)."""
+    from curtree_b200 import datasets as D
+    b = D.uniform_boxes(10_000_000, seed=3)
+    return b, D.uniform_windows(1_000_000, seed=113, max_side=1e-3)
+
+
+def small_windows_leg(args, C, stream, reps=3):
+    """The small-windows batch through the drop-in calls (crt_build_f32 in
+    place, crt_query_f32 allocating the pairs; fanout 10, the reference's
+    default), median of `reps` queries, every window checked against the
+    oracle's tree query on the oracle's own build."""
+    import torch
+    b, q = small_windows_case()
+    d = C.BBox.from_host(b)
+    rt = C.RTree(10)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    C.build_rtree(d, rt, stream)
+    e1.record(stream)
+    e1.synchronize()
+    build_ms = e0.elapsed_time(e1)
+    dq = C.BBox.from_host(q)
+    qms = []
+    dg = None
+    for r in range(reps + 1):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pr = C.bfs_frontier(rt, d, dq, stream)
+        e1.record(stream)
+        e1.synchronize()
+        if r:
+            qms.append(e0.elapsed_time(e1))
+        if r == reps and args.parity:
+            g = C.PairDigest(q.n)
+            g.add_ptr(pr.s.fid, pr.s.tid, pr.sz)
+            dg = g.to_host()
+        npairs = pr.sz
+        pr.free()
+    out = {"workload": "10M uniform boxes (side U[0,1e-3]) x 1M windows (side U[0,1e-3]), fanout 10; "
+                       "crt_build_f32 + crt_query_f32 (drop-in)",
+           "build_ms": build_ms, "query_ms": statistics.median(qms), "pairs": int(npairs),
+           "windows_per_s": q.n / (statistics.median(qms) / 1e3)}
+    if dg is not None:
+        from oracle import oracle as O
+        sb, tr, same = oracle_tree(b, 10, rt, d)
+        want = O.tree_query_stats(tr, sb, q)
+        cmp = compare_digests(dg[0], dg[1], want.counts, want.hashes)
+        out["parity"] = dict(cmp, ok=bool(cmp["digest_ok"] and same and dg[2] == 0), tree_identical=same)
+    rt.free()
+    return out
+
+
 def config1_leg(args, C, stream, reps=10):
     """The reference's own small case: 1M uniform boxes (side U[0,1e-3]),
     10k windows (side U[0,1e-2]), fanout 10, through the drop-in calls a
@@ -1261,7 +1320,9 @@ def reference_gpu_leg():
                  ("build_100M_clustered", lambda: D.clustered_boxes(100_000_000, seed=2),
                   None, 10, 3),
                  ("batched_10M_x_1M", lambda: D.uniform_boxes(10_000_000, seed=3),
-                  lambda b: D.mixed_windows(1_000_000, b, seed=103), 10, 1)]
+                  lambda b: D.mixed_windows(1_000_000, b, seed=103), 10, 1),
+                 ("small_windows_10M_x_1M", lambda: small_windows_case()[0],
+                  lambda b: small_windows_case()[1], 10, 3)]
         for name, mk_b, mk_q, f, reps in cases:
             b = mk_b()
             bfile = os.path.join(tmp, name + "_b.crtb")
@@ -1367,7 +1428,7 @@ def main():
                   "ingest": out.get("ingest"), "cpu_rtree": out.get("cpu_rtree"),
                   "workload_stats": out["workload_stats"], "autotune": out.get("autotune"),
                   "parity": out.get("parity"), "e2e": out.get("e2e"), "roofline": out["roofline"],
-                  "config1": out.get("config1")}
+                  "config1": out.get("config1"), "small_windows": out.get("small_windows")}
         if args.detail:
             with open(args.detail, "w") as f:
                 json.dump(detail, f, indent=1)
@@ -1438,6 +1499,10 @@ def compact_legs(out):
     if c1:
         o["config1"] = {"build_ms": _r(c1["build_ms"]), "query_ms": _r(c1["query_ms"]),
                         "pairs": c1["pairs"]}
+    sw = out.get("small_windows")
+    if sw:
+        o["small_windows"] = {"build_ms": _r(sw["build_ms"]), "query_ms": _r(sw["query_ms"]),
+                              "pairs": sw["pairs"]}
     bd = out.get("build")
     if bd:
         o["build"] = {"boxes_per_s": _r(bd["value"], 0), "ms_per_step": _r(bd["ms_per_step"]),
@@ -1462,6 +1527,9 @@ def compact_parity(out):
     c1 = (out.get("config1") or {}).get("parity")
     if c1:
         p["config1"] = {"ok": c1["ok"], "windows": c1["windows"], "pairs": c1["pairs"]}
+    sw = (out.get("small_windows") or {}).get("parity")
+    if sw:
+        p["small_windows"] = {"ok": sw["ok"], "windows": sw["windows"], "pairs": sw["pairs"]}
     v = (out.get("adversarial") or {}).get("parity")
     if v:
         p["adversarial"] = {"ok": v["ok"], "tree_identical": v["tree_identical"],
