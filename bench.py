@@ -199,32 +199,39 @@ def cpu_reference_rate(boxes, windows, seconds: float, rng_seed: int = 7, keep=F
     return (out, kept) if keep else out
 
 
-def cpu_rtree_rate(h_tree, h_sorted, windows, seconds: float, rng_seed: int = 9):
-    """Windows/s of a CPU R-tree on all host threads: the same packed tree
-    (the reference's layout, copied from the device) searched depth-first by
-    the oracle's C restatement of the reference's tree query, counting hits
-    and pair digests without writing pairs.  It stands in for the reference's
-    Boost R-tree check (src/verify.hpp:35-104), whose Boost dependency is
-    absent; a sample of windows sized to about `seconds` of CPU work."""
+def cpu_rtree_rate(boxes, windows, seconds: float, rng_seed: int = 9):
+    """Windows/s of a CPU R-tree on all host threads, as the reference's CPU
+    check runs one (src/verify.hpp:35-95: Boost's rtree<value,
+    quadratic<16>>, built by inserting the boxes one at a time, then queried
+    window by window).  Boost is absent, so the index is the oracle's
+    restatement of that algorithm (Guttman's quadratic split, 4-16 entries
+    per node), built over the same boxes on one thread; the queries run on
+    all host threads over a sample of windows sized to about `seconds` of
+    CPU work, and their pairs are counted and digested."""
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(rng_seed)
+    tree = O.QuadraticRTree(boxes)
 
     def run(m):
         idx = np.sort(rng.choice(windows.n, size=min(m, windows.n), replace=False))
         q = windows.take(idx)
-        t0 = time.perf_counter()
-        st = O.tree_query_stats(h_tree, h_sorted, q, nthreads=threads)
-        return q.n, time.perf_counter() - t0, st.total
+        c, h, t = tree.query_stats(q, qid=idx.astype(np.int32), nthreads=threads)
+        return q.n, t, int(c.sum()), (idx, c, h)
 
-    n0, t0, _ = run(threads * 8)
+    n0, t0, _, _ = run(threads * 8)
     m = int(max(threads, min(windows.n, n0 / max(t0, 1e-6) * seconds)))
     m = (m + threads - 1) // threads * threads
-    n, t, pairs = run(m)
+    n, t, pairs, kept = run(m)
+    build_s = tree.build_seconds
+    tree.free()
     return {"value": n / t, "unit": "windows/s", "cores": threads, "kind": "port",
-            "sample": f"{n} of {windows.n} windows x {h_sorted.n} boxes, {t:.1f} s, {pairs} pairs",
-            "what": "depth-first search of the same packed tree on the host (oracle restatement "
-                    "of the reference's query), hits counted, no pair writes"}
+            "build_s": build_s,
+            "sample": f"{n} of {windows.n} windows x {boxes.n} boxes, {t:.1f} s, {pairs} pairs",
+            "what": "Guttman R-tree with the quadratic split, 4-16 entries per node, built by "
+                    "inserting the boxes one at a time on one thread (the index of the "
+                    "reference's Boost check, restated: Boost is absent); queries on all host "
+                    "threads"}, kept
 
 
 # ---------------------------------------------------------------------------
@@ -505,8 +512,11 @@ def run_ours(args, rank, world, dist):
     # ---- CPU R-tree on the same tree (rank 0 of a 1-GPU run) ------------------
     if "cpu" not in skip and rank == 0 and world == 1:
         try:
-            out["cpu_rtree"] = cpu_rtree_rate(rt.to_host(), sorted_box.to_host(), windows,
-                                              args.cpu_seconds)
+            out["cpu_rtree"], (idx, qc, qh) = cpu_rtree_rate(boxes, windows, args.cpu_seconds)
+            if "persistent" in digests:
+                c, h, _ = digests["persistent"]
+                out["cpu_rtree"]["same_pairs_as_gpu"] = bool(np.array_equal(c[idx], qc) and
+                                                             np.array_equal(h[idx], qh))
         except Exception as e:  # a side figure: report it, keep the line
             out["cpu_rtree"] = {"error": f"{type(e).__name__}: {e}"}
 
@@ -1466,8 +1476,10 @@ def compact_legs(out):
     """The sub-legs in a few keys each, so the end of the line carries them;
     the full figures go to the detail record."""
     o = {}
-    if out.get("cpu_rtree") and "value" in out["cpu_rtree"]:
-        o["cpu_rtree_windows_per_s"] = _r(out["cpu_rtree"]["value"], 1)
+    cr = out.get("cpu_rtree")
+    if cr and "value" in cr:
+        o["cpu_rtree"] = {"windows_per_s": _r(cr["value"], 1), "build_s": _r(cr["build_s"], 2),
+                          "same_pairs_as_gpu": cr.get("same_pairs_as_gpu")}
     a = out.get("autotune")
     if a:
         o["autotune"] = {"chosen": a["chosen"], "rows": len(a["table"]),

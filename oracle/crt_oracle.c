@@ -26,6 +26,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 /* ------------------------------------------------------------------------ */
 /* Morton key                                                                */
@@ -520,4 +521,289 @@ int64_t orc_nested_loop_pairs(const float* qxmin, const float* qymin, const floa
     }
   }
   return n;
+}
+
+/* ---------------------------------------------------------------------------
+ * The reference's CPU check builds a Boost.Geometry rtree<value,
+ * quadratic<16>> by inserting the boxes one at a time and then queries it
+ * box by box (src/verify.hpp:35-95).  Boost is not available here, so this
+ * restates the algorithm that parameter set names: Guttman's R-tree with the
+ * quadratic split (A. Guttman, "R-trees: a dynamic index structure for
+ * spatial searching", SIGMOD 1984), at most 16 and at least 4 entries per
+ * node (Boost's default minimum for quadratic<16> is 0.3 x 16).  Insertion
+ * descends to the child needing the least area enlargement (ties: the
+ * smaller area), splits an overflowing node by the quadratic method (seeds:
+ * the pair wasting the most area; then the entry with the greatest
+ * preference for one group, to the group it enlarges least, keeping every
+ * group at the minimum), and adjusts the covering rectangles up the path.
+ * CPU baseline only: its tree shape differs from the reference's packed
+ * tree, its pair set is the brute force's.
+ * ------------------------------------------------------------------------- */
+#define QR_MAX 16
+#define QR_MIN 4
+
+typedef struct { float x0, y0, x1, y1; } qr_rect;
+
+typedef struct qr_node {
+  int leaf, n;
+  qr_rect r[QR_MAX + 1];
+  intptr_t ent[QR_MAX + 1]; /* child node, or box id in a leaf */
+} qr_node;
+
+typedef struct {
+  qr_node* root;
+  int height;
+  qr_node** blocks;
+  int64_t nblocks, cap_blocks, used; /* nodes handed out of the last block */
+} qr_tree;
+
+#define QR_BLOCK 65536
+
+static qr_node* qr_alloc(qr_tree* t, int leaf)
+{
+  if (t->nblocks == 0 || t->used == QR_BLOCK) {
+    if (t->nblocks == t->cap_blocks) {
+      int64_t c = t->cap_blocks ? 2 * t->cap_blocks : 64;
+      qr_node** b = (qr_node**)realloc(t->blocks, sizeof(qr_node*) * (size_t)c);
+      if (!b) return NULL;
+      t->blocks = b;
+      t->cap_blocks = c;
+    }
+    qr_node* blk = (qr_node*)malloc(sizeof(qr_node) * QR_BLOCK);
+    if (!blk) return NULL;
+    t->blocks[t->nblocks++] = blk;
+    t->used = 0;
+  }
+  qr_node* nd = &t->blocks[t->nblocks - 1][t->used++];
+  nd->leaf = leaf;
+  nd->n = 0;
+  return nd;
+}
+
+static inline float qr_area(qr_rect a) { return (a.x1 - a.x0) * (a.y1 - a.y0); }
+static inline qr_rect qr_union(qr_rect a, qr_rect b)
+{
+  qr_rect u = {a.x0 < b.x0 ? a.x0 : b.x0, a.y0 < b.y0 ? a.y0 : b.y0, a.x1 > b.x1 ? a.x1 : b.x1,
+               a.y1 > b.y1 ? a.y1 : b.y1};
+  return u;
+}
+static qr_rect qr_cover(const qr_node* nd)
+{
+  qr_rect u = nd->r[0];
+  for (int i = 1; i < nd->n; i++) u = qr_union(u, nd->r[i]);
+  return u;
+}
+
+/* Splits the QR_MAX + 1 entries of nd between nd and a new node (quadratic). */
+static qr_node* qr_split(qr_tree* t, qr_node* nd)
+{
+  const int m = nd->n;
+  qr_rect r[QR_MAX + 1];
+  intptr_t e[QR_MAX + 1];
+  memcpy(r, nd->r, sizeof(qr_rect) * (size_t)m);
+  memcpy(e, nd->ent, sizeof(intptr_t) * (size_t)m);
+  int s1 = 0, s2 = 1;
+  float worst = -INFINITY;
+  for (int i = 0; i < m; i++)
+    for (int j = i + 1; j < m; j++) {
+      const float d = qr_area(qr_union(r[i], r[j])) - qr_area(r[i]) - qr_area(r[j]);
+      if (d > worst) { worst = d; s1 = i; s2 = j; }
+    }
+  qr_node* b = qr_alloc(t, nd->leaf);
+  if (!b) return NULL;
+  char done[QR_MAX + 1];
+  memset(done, 0, sizeof(done));
+  nd->n = 0;
+  nd->r[0] = r[s1]; nd->ent[0] = e[s1]; nd->n = 1;
+  b->r[0] = r[s2]; b->ent[0] = e[s2]; b->n = 1;
+  done[s1] = done[s2] = 1;
+  qr_rect ca = r[s1], cb = r[s2];
+  int left = m - 2;
+  while (left > 0) {
+    qr_node* all = NULL;
+    if (nd->n + left == QR_MIN) all = nd;
+    else if (b->n + left == QR_MIN) all = b;
+    if (all) {
+      for (int k = 0; k < m; k++)
+        if (!done[k]) { all->r[all->n] = r[k]; all->ent[all->n] = e[k]; all->n++; done[k] = 1; }
+      break;
+    }
+    int pick = -1;
+    float best = -1.f, pd1 = 0.f, pd2 = 0.f;
+    for (int k = 0; k < m; k++) {
+      if (done[k]) continue;
+      const float d1 = qr_area(qr_union(ca, r[k])) - qr_area(ca);
+      const float d2 = qr_area(qr_union(cb, r[k])) - qr_area(cb);
+      const float diff = fabsf(d1 - d2);
+      if (pick < 0 || diff > best) { best = diff; pick = k; pd1 = d1; pd2 = d2; }
+    }
+    int to_a;
+    if (pd1 != pd2) to_a = pd1 < pd2;
+    else if (qr_area(ca) != qr_area(cb)) to_a = qr_area(ca) < qr_area(cb);
+    else to_a = nd->n <= b->n;
+    qr_node* g = to_a ? nd : b;
+    g->r[g->n] = r[pick]; g->ent[g->n] = e[pick]; g->n++;
+    if (to_a) ca = qr_union(ca, r[pick]); else cb = qr_union(cb, r[pick]);
+    done[pick] = 1;
+    left--;
+  }
+  return b;
+}
+
+static int qr_insert(qr_tree* t, qr_rect rc, int id)
+{
+  qr_node* path[64];
+  int slot[64];
+  int d = 0;
+  qr_node* nd = t->root;
+  while (!nd->leaf) {
+    int best = 0;
+    float be = INFINITY, ba = INFINITY;
+    for (int i = 0; i < nd->n; i++) {
+      const float a = qr_area(nd->r[i]);
+      const float en = qr_area(qr_union(nd->r[i], rc)) - a;
+      if (en < be || (en == be && a < ba)) { be = en; ba = a; best = i; }
+    }
+    path[d] = nd; slot[d] = best; d++;
+    nd = (qr_node*)nd->ent[best];
+  }
+  nd->r[nd->n] = rc; nd->ent[nd->n] = id; nd->n++;
+  qr_node* split = NULL;
+  if (nd->n > QR_MAX && !(split = qr_split(t, nd))) return -2;
+  qr_node* child = nd;
+  while (d > 0) {
+    d--;
+    qr_node* p = path[d];
+    p->r[slot[d]] = qr_cover(child);
+    if (split) {
+      p->r[p->n] = qr_cover(split); p->ent[p->n] = (intptr_t)split; p->n++;
+      split = NULL;
+      if (p->n > QR_MAX && !(split = qr_split(t, p))) return -2;
+    }
+    child = p;
+  }
+  if (split) {  /* the root split: a new root over both halves */
+    qr_node* r = qr_alloc(t, 0);
+    if (!r) return -2;
+    r->r[0] = qr_cover(t->root); r->ent[0] = (intptr_t)t->root;
+    r->r[1] = qr_cover(split); r->ent[1] = (intptr_t)split;
+    r->n = 2;
+    t->root = r;
+    t->height++;
+  }
+  return 0;
+}
+
+static double qr_now(void)
+{
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+/* Inserts the n boxes in input order; *seconds receives the build time. */
+void* orc_qrtree_build(const float* xmin, const float* ymin, const float* xmax, const float* ymax,
+                       const int32_t* id, int64_t n, double* seconds)
+{
+  const double t0 = qr_now();
+  qr_tree* t = (qr_tree*)calloc(1, sizeof(qr_tree));
+  if (!t) return NULL;
+  t->root = qr_alloc(t, 1);
+  t->height = 1;
+  for (int64_t i = 0; i < n && t->root; i++) {
+    qr_rect rc = {xmin[i], ymin[i], xmax[i], ymax[i]};
+    if (qr_insert(t, rc, id[i]) != 0) { t->root = NULL; break; }
+  }
+  if (seconds) *seconds = qr_now() - t0;
+  return t;
+}
+
+void orc_qrtree_free(void* h)
+{
+  qr_tree* t = (qr_tree*)h;
+  if (!t) return;
+  for (int64_t b = 0; b < t->nblocks; b++) free(t->blocks[b]);
+  free(t->blocks);
+  free(t);
+}
+
+typedef struct {
+  const qr_tree* t;
+  const float *qx0, *qy0, *qx1, *qy1;
+  const int32_t* qid;
+  int64_t q0, q1;
+  int64_t* counts;
+  uint64_t* hashes;
+  int status;
+} qr_args;
+
+static void* qr_query_worker(void* p)
+{
+  qr_args* a = (qr_args*)p;
+  const int cap = 64 * QR_MAX;
+  const qr_node** st = (const qr_node**)malloc(sizeof(qr_node*) * (size_t)cap);
+  if (!st) { a->status = -2; return NULL; }
+  for (int64_t q = a->q0; q < a->q1; q++) {
+    const float x1 = a->qx0[q], y1 = a->qy0[q], x2 = a->qx1[q], y2 = a->qy1[q];
+    const int32_t qo = a->qid ? a->qid[q] : (int32_t)q;
+    int64_t cnt = 0;
+    uint64_t h = 0;
+    int sp = 0;
+    st[sp++] = a->t->root;
+    while (sp > 0) {
+      const qr_node* nd = st[--sp];
+      for (int i = 0; i < nd->n; i++) {
+        const qr_rect r = nd->r[i];
+        if (!isect(x1, y1, x2, y2, r.x0, r.y0, r.x1, r.y1)) continue;
+        if (nd->leaf) {
+          cnt++;
+          h += orc_pair_hash(qo, (int32_t)nd->ent[i]);
+        } else if (sp < cap) {
+          st[sp++] = (const qr_node*)nd->ent[i];
+        } else {
+          a->status = -3;
+        }
+      }
+    }
+    if (a->counts) a->counts[q] = cnt;
+    if (a->hashes) a->hashes[q] = h;
+  }
+  free(st);
+  return NULL;
+}
+
+/* Per-window counts and pair digests over `nthreads` host threads (the tree
+ * is read-only); *seconds receives the wall time of the queries. */
+int orc_qrtree_query_stats(void* h, const float* qxmin, const float* qymin, const float* qxmax,
+                           const float* qymax, const int32_t* qid, int64_t nq, int64_t* counts,
+                           uint64_t* hashes, int nthreads, double* seconds)
+{
+  qr_tree* t = (qr_tree*)h;
+  if (!t || !t->root) return -1;
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  pthread_t th[256];
+  qr_args args[256];
+  int started[256];
+  const double t0 = qr_now();
+  const int64_t per = (nq + nthreads - 1) / nthreads;
+  for (int i = 0; i < nthreads; i++) {
+    qr_args* a = &args[i];
+    memset(a, 0, sizeof(*a));
+    a->t = t;
+    a->qx0 = qxmin; a->qy0 = qymin; a->qx1 = qxmax; a->qy1 = qymax; a->qid = qid;
+    a->q0 = i * per; a->q1 = (i + 1) * per < nq ? (i + 1) * per : nq;
+    a->counts = counts; a->hashes = hashes;
+    started[i] = 0;
+    if (a->q0 >= a->q1) continue;
+    if (pthread_create(&th[i], NULL, qr_query_worker, a) == 0) started[i] = 1;
+    else qr_query_worker(a);
+  }
+  int st = 0;
+  for (int i = 0; i < nthreads; i++) {
+    if (started[i]) pthread_join(th[i], NULL);
+    if (args[i].status != 0) st = args[i].status;
+  }
+  if (seconds) *seconds = qr_now() - t0;
+  return st;
 }

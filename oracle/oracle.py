@@ -70,6 +70,14 @@ def lib():
         L.orc_nested_loop_stats.argtypes = nl_args + [_i64p, _u64p, ctypes.c_int]
         L.orc_nested_loop_pairs.restype = _i64
         L.orc_nested_loop_pairs.argtypes = nl_args + [_i32p, _i32p, _i64]
+        L.orc_qrtree_build.restype = ctypes.c_void_p
+        L.orc_qrtree_build.argtypes = [_f32p] * 4 + [_i32p, _i64, ctypes.POINTER(ctypes.c_double)]
+        L.orc_qrtree_free.restype = None
+        L.orc_qrtree_free.argtypes = [ctypes.c_void_p]
+        L.orc_qrtree_query_stats.restype = ctypes.c_int
+        L.orc_qrtree_query_stats.argtypes = [ctypes.c_void_p] + [_f32p] * 4 + [ctypes.c_void_p, _i64,
+                                                                                _i64p, _u64p, ctypes.c_int,
+                                                                                ctypes.POINTER(ctypes.c_double)]
         L.orc_pair_hash.restype = ctypes.c_uint64
         L.orc_pair_hash.argtypes = [ctypes.c_int32, ctypes.c_int32]
         _lib = L
@@ -286,6 +294,47 @@ def ref_nested_loop_digest(q, d, qid, nthreads: int | None = None):
                                                   *_box_args(d), _c(d.id, np.int32), d.n,
                                                   nthreads, counts, hashes, ctypes.byref(secs))
     return counts[:q.n], hashes[:q.n], int(n), secs.value
+
+
+class QuadraticRTree:
+    """The reference's CPU check's index (src/verify.hpp:35-95: Boost's
+    rtree<value, quadratic<16>>, built by inserting the boxes one at a time),
+    restated: Guttman's R-tree with the quadratic split, 4-16 entries per
+    node (orc_qrtree_* in crt_oracle.c).  Boost is not available here."""
+
+    def __init__(self, boxes):
+        secs = ctypes.c_double(0)
+        self._keep = [_c(a, np.float32) for a in (boxes.xmin, boxes.ymin, boxes.xmax, boxes.ymax)]
+        self._id = _c(boxes.id, np.int32)
+        self.h = lib().orc_qrtree_build(*self._keep, self._id, boxes.n, ctypes.byref(secs))
+        if not self.h:
+            raise MemoryError("quadratic R-tree build failed")
+        self.build_seconds = secs.value
+
+    def query_stats(self, q, qid=None, nthreads: int | None = None):
+        """(counts, digests, seconds of the queries) for the windows q."""
+        nthreads = nthreads or os.cpu_count() or 1
+        counts = np.zeros(max(q.n, 1), np.int64)
+        hashes = np.zeros(max(q.n, 1), np.uint64)
+        ids = _c(qid, np.int32) if qid is not None else None
+        secs = ctypes.c_double(0)
+        rc = lib().orc_qrtree_query_stats(self.h, *_box_args(q),
+                                          ids.ctypes.data if ids is not None else None, q.n,
+                                          counts, hashes, nthreads, ctypes.byref(secs))
+        if rc != 0:
+            raise RuntimeError(f"quadratic R-tree query failed ({rc})")
+        return counts[:q.n], hashes[:q.n], secs.value
+
+    def free(self):
+        if self.h:
+            lib().orc_qrtree_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def ref_read_mbr(path: str, n: int, r: float):

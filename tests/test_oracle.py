@@ -192,3 +192,21 @@ def test_oracle_query_matches_reference_golden(path):
     # and the brute force agrees (no NaN in query fixtures)
     did, qid = O.nested_loop_pairs(q, b)
     assert np.array_equal(fid, did) and np.array_equal(tid, qid)
+
+
+def test_quadratic_rtree_matches_brute_force():
+    """The CPU R-tree of the reference's Boost check, restated (Guttman's
+    quadratic split, 4-16 entries per node, built by insertion): every
+    window's pair count and digest equal the brute force's, on uniform and
+    clustered boxes with duplicates and points, with window ids."""
+    from curtree_b200 import datasets as D
+    for b in (D.uniform_boxes(60_000, seed=31), D.clustered_boxes(60_000, seed=32, chunk=60_000)):
+        q = D.mixed_windows(3000, b, seed=131)
+        t = O.QuadraticRTree(b)
+        ids = np.arange(5, 5 + q.n, dtype=np.int32)
+        c, h, _ = t.query_stats(q, qid=ids, nthreads=4)
+        t.free()
+        fid, qo = O.nested_loop_pairs(q, b)
+        wc, wh = O.pair_hashes(fid, ids[qo], 5 + q.n)
+        assert c.sum() > 10_000
+        assert np.array_equal(c, wc[5:]) and np.array_equal(h, wh[5:])
