@@ -517,7 +517,7 @@ constexpr int kLevelChunk = 2048;  // children staged per round
 // gathered from the AoS copy through the sorted slot order, and the permuted
 // SoA is written on the way; otherwise children are nodes at child_start.
 template <bool kLeaf>
-__global__ void __launch_bounds__(kLevelThreads)
+__global__ void __launch_bounds__(kLevelThreads, 3)  // 80 registers: three CTAs per SM
     level_kernel(int nodes_per_cta, int fanout, int64_t nchild, int64_t nparent,
                  int64_t parent_start, int64_t pos_base,
                  // leaf inputs/outputs
