@@ -81,8 +81,8 @@ static std::atomic<double> g_pairs_per_window{64.0};
 
 // The drop-in query runs into a working buffer from the stream-ordered pool
 // (sized from the last call's pairs per window, re-run once at the exact size
-// if that was too small), then copies the pairs into exact-size cudaMalloc
-// arrays, which the caller frees with cudaFree as the reference's
+// if that was too small), then copies the pairs into two exact-size arrays
+// from the same pool, which the caller frees with cudaFree as the reference's
 // idpair_d_free does (src/utility.cuh:164-195).  Batches below
 // kDropinPersistentMin windows take the plain form: its fixed cost (no
 // window sort, no chunk compaction) is far below the persistent form's,
@@ -140,7 +140,11 @@ static int query_dropin(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   int32_t *fid = nullptr, *tid = nullptr;
   if (rc == CRT_OK) {
     const size_t bytes = sizeof(int32_t) * (size_t)std::max<int64_t>(h.count, 1);
-    if (cudaMalloc((void**)&fid, bytes) != cudaSuccess || cudaMalloc((void**)&tid, bytes) != cudaSuccess) {
+    // two allocations, as idpair_d_alloc makes them, from the device's
+    // stream-ordered pool: cudaFree (the reference's idpair_d_free) accepts
+    // them, and they cost no device-wide synchronisation here
+    if (cudaMallocAsync((void**)&fid, bytes, stream) != cudaSuccess ||
+        cudaMallocAsync((void**)&tid, bytes, stream) != cudaSuccess) {
       cudaGetLastError();
       rc = fail(CRT_ERR_OOM, "query: output allocation failed");
     } else if (h.count > 0) {
@@ -154,8 +158,9 @@ static int query_dropin(const crt_rtree_f32* d_rt, const crt_bbox_f32* d_rbox,
   cudaError_t e = cudaStreamSynchronize(stream);
   if (rc == CRT_OK && e != cudaSuccess) rc = cuda_fail(e, "query: copy");
   if (rc != CRT_OK) {
-    if (fid) cudaFree(fid);
-    if (tid) cudaFree(tid);
+    if (fid) cudaFreeAsync(fid, stream);
+    if (tid) cudaFreeAsync(tid, stream);
+    cudaStreamSynchronize(stream);
     return rc;
   }
   if (nq > 0) g_pairs_per_window.store(std::max(1.0, (double)h.count / (double)nq));
@@ -219,7 +224,10 @@ int crt_build_f32(crt_bbox_f32* d_box, crt_rtree_f32* d_rt, crt_stream_t stream,
   if (rsz < 0) return fail(CRT_ERR_INVALID_ARG, "build: need sz >= 1 and fanout >= 2");
   if (n + rsz > INT32_MAX) return fail(CRT_ERR_INVALID_ARG, "build: sz + R_sz exceeds INT32_MAX");
   init_device();
-  // node arrays: cudaMalloc, as rt_d_alloc does (src/utility.cuh:114-135)
+  // node arrays: six allocations, as rt_d_alloc makes them
+  // (src/utility.cuh:114-135), from the device's stream-ordered pool:
+  // cudaFree (the reference's rt_d_free) accepts them; build_tree synchronises
+  // the stream before this returns
   crt_rtree_f32 t = *d_rt;
   t.sz = (int)rsz;
   t.xmin = t.ymin = t.xmax = t.ymax = nullptr;
@@ -228,9 +236,10 @@ int crt_build_f32(crt_bbox_f32* d_box, crt_rtree_f32* d_rt, crt_stream_t stream,
     void** arr[6] = {(void**)&t.xmin, (void**)&t.ymin, (void**)&t.xmax, (void**)&t.ymax,
                      (void**)&t.pos, (void**)&t.len};
     for (int a = 0; a < 6; a++) {
-      if (cudaMalloc(arr[a], sizeof(float) * (size_t)rsz) != cudaSuccess) {
+      if (cudaMallocAsync(arr[a], sizeof(float) * (size_t)rsz, (cudaStream_t)stream) != cudaSuccess) {
         cudaGetLastError();
-        for (int b = 0; b < a; b++) cudaFree(*arr[b]);
+        for (int b = 0; b < a; b++) cudaFreeAsync(*arr[b], (cudaStream_t)stream);
+        cudaStreamSynchronize((cudaStream_t)stream);
         return fail(CRT_ERR_OOM, "build: node allocation failed");
       }
     }

@@ -92,8 +92,8 @@ uint64_t crt_kernel_launches(void);
  * (src/rtree_bulkload_thrust.cuh:62-213).
  * Reads d_rt->fanout, sorts d_box IN PLACE into Z-order (its five arrays are
  * permuted; id[] then holds the original ids), allocates the six node arrays
- * of d_rt with cudaMalloc (free with crt_rtree_free or the reference's
- * rt_d_free), fills them bit-exactly as the reference does, sets d_rt->sz and
+ * of d_rt from the device's stream-ordered pool (cudaMallocAsync on stream;
+ * free with crt_rtree_free or the reference's rt_d_free, both cudaFree), fills them bit-exactly as the reference does, sets d_rt->sz and
  * *out_r_sz to R_sz.  Returns after the tree is complete on the device.
  * d_box->sz == 1 gives R_sz == 0, as in the reference; d_box->sz < 1 or
  * fanout < 2 (where the reference never returns) give CRT_ERR_INVALID_ARG. */
@@ -103,8 +103,8 @@ int crt_build_f32(crt_bbox_f32* d_box, crt_rtree_f32* d_rt, crt_stream_t stream,
 /* Replaces `bfs_frontier(const RTREE<T>&, const BBOX<T>& d_rbox,
  * const BBOX<T>& d_qbox, IDPAIR& d_dq)` (src/rtree_bfs_frontier.cuh:292-529).
  * d_rbox is the box set build sorted (same arrays as d_box after
- * crt_build_f32).  Allocates d_dq->fid / d_dq->tid with cudaMalloc (free with
- * crt_idpair_free or the reference's idpair_d_free) and fills them with every
+ * crt_build_f32).  Allocates d_dq->fid / d_dq->tid from the stream-ordered
+ * pool (free with crt_idpair_free or the reference's idpair_d_free) and fills them with every
  * (box id, query index) pair whose boxes intersect, in unspecified order.
  * Never overflows (the reference aborts when a 32-query block expands past
  * 1024 nodes); results past INT32_MAX pairs give CRT_ERR_OVERFLOW_INT32.
