@@ -780,6 +780,7 @@ static TreeView make_view(const crt_rtree_f32& rt, const crt_bbox_f32& rb)
   T.nlev = 0;
   T.lvl_first = nullptr;
   T.lvl_span = nullptr;
+  T.lvl_odd = nullptr;
   return T;
 }
 
@@ -819,18 +820,45 @@ __global__ void write_levels_kernel(LevelTables t, int* __restrict__ first,
   }
 }
 
-// Puts the tables at `dev` (kLevelTableBytes, 8-byte aligned) and points the
-// view at them.
+// *odd = 1 when some box is not ordinary (*odd was zeroed before).  Every
+// thread that sees one stores the same value.
+__global__ void __launch_bounds__(256)
+    odd_boxes_kernel(const float* __restrict__ xmin, const float* __restrict__ ymin,
+                     const float* __restrict__ xmax, const float* __restrict__ ymax, int64_t n,
+                     int* __restrict__ odd)
+{
+  bool bad = false;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    bad |= !(xmin[i] <= xmax[i] && ymin[i] <= ymax[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) *odd = 1;
+}
+
+void launch_odd_boxes(const float* xmin, const float* ymin, const float* xmax, const float* ymax,
+                      int64_t n, int* odd, cudaStream_t stream)
+{
+  cudaMemsetAsync(odd, 0, sizeof(int), stream);
+  if (n <= 0) return;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(cdiv(n, 256), (int64_t)sm_count() * 8));
+  odd_boxes_kernel<<<grid, 256, 0, stream>>>(xmin, ymin, xmax, ymax, n, odd);
+  CRT_LAUNCHED(1);
+}
+
+// Puts the tables at `dev` (kLevelTableBytes, 8-byte aligned), checks the
+// view's boxes for the shortcut and points the view at both.
 static void attach_levels(TreeView& T, const LevelTables& t, void* dev, cudaStream_t stream)
 {
   if (t.nlev == 0) return;
   int* first = (int*)dev;
   long long* span = (long long*)((char*)dev + sizeof(int) * kMaxLevels);
+  int* odd = (int*)((char*)dev + kLevelOddOffset);
   write_levels_kernel<<<1, 64, 0, stream>>>(t, first, span);
   CRT_LAUNCHED(1);
+  launch_odd_boxes(T.bxmin, T.bymin, T.bxmax, T.bymax, T.nbox, odd, stream);
   T.nlev = t.nlev;
   T.lvl_first = first;
   T.lvl_span = span;
+  T.lvl_odd = odd;
 }
 
 // Number of levels of a tree with R_sz nodes over nbox boxes at this fanout

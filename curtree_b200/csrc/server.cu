@@ -66,6 +66,7 @@ struct SrvTree {
   int nlev;  // containment tables (nlev == 0: off)
   const int* lvl_first;
   const long long* lvl_span;
+  const int* lvl_odd;  // set: some box is not ordinary (shortcut off)
 };
 
 struct SrvDesc {
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(kSrvThreads)
     T.bxmin = tr.bxmin; T.bymin = tr.bymin; T.bxmax = tr.bxmax; T.bymax = tr.bymax;
     T.bid = tr.bid; T.nbox = tr.nbox;
     T.nlev = tr.nlev; T.lvl_first = tr.lvl_first; T.lvl_span = tr.lvl_span;
+    T.lvl_odd = tr.lvl_odd;
     int lg, lc;
     lane_map(T.fanout, tr.K, lg, lc);
     SrvCtr* ctr = &ctrs[r % slots];
@@ -759,9 +761,14 @@ int crt_server_add_tree(crt_server h, const crt_rtree_f32* rt, const crt_bbox_f3
     cudaMemcpy(dev + sizeof(int) * kMaxLevels, lt.span, sizeof(long long) * kMaxLevels,
                cudaMemcpyHostToDevice);
     s->tables.push_back(dev);
+    launch_odd_boxes(rbox->xmin, rbox->ymin, rbox->xmax, rbox->ymax, rbox->sz,
+                     (int*)(dev + kLevelOddOffset), 0);
+    const cudaError_t e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) return cuda_fail(e, "server_add_tree");
     t.nlev = lt.nlev;
     t.lvl_first = (const int*)dev;
     t.lvl_span = (const long long*)(dev + sizeof(int) * kMaxLevels);
+    t.lvl_odd = (const int*)(dev + kLevelOddOffset);
   }
   TreeStats ts;
   if (rt->sz > 0 && rbox->sz > 0) {

@@ -48,18 +48,27 @@ struct TreeView {
   int nlev;
   const int* __restrict__ lvl_first;        // first node index of height h
   const long long* __restrict__ lvl_span;   // boxes under a full node of height h
+  // Non-zero word: some box is not ordinary, and the shortcut is off (null:
+  // every box was found ordinary when the tables were made).
+  const int* __restrict__ lvl_odd;
 };
 
 // Host image of the containment tables: kMaxLevels ints (first node of each
-// height) then kMaxLevels int64 (boxes under a full node of that height).
+// height) then kMaxLevels int64 (boxes under a full node of that height).  On
+// the device a flag word follows them: set when some box is not ordinary.
 struct LevelTables {
   int nlev = 0;
   int first[kMaxLevels];
   long long span[kMaxLevels];
 };
-constexpr size_t kLevelTableBytes = sizeof(int) * kMaxLevels + sizeof(long long) * kMaxLevels;
+constexpr size_t kLevelOddOffset = sizeof(int) * kMaxLevels + sizeof(long long) * kMaxLevels;
+constexpr size_t kLevelTableBytes = kLevelOddOffset + 16;
 // Tables of a tree in the reference's packed layout; nlev == 0 otherwise.
 LevelTables level_tables(const crt_rtree_f32& rt, int64_t nbox);
+// Zeroes *odd, then sets it when some of the n boxes is not ordinary
+// (xmin <= xmax and ymin <= ymax, which a NaN coordinate also fails).
+void launch_odd_boxes(const float* xmin, const float* ymin, const float* xmax, const float* ymax,
+                      int64_t n, int* odd, cudaStream_t stream);
 
 struct WindowView {
   const float* __restrict__ xmin;
@@ -214,11 +223,15 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
     }
     return;
   }
-  // A window that contains a node's MBR hits every box under it (each box
-  // lies inside the node's MBR; a NaN box coordinate never excludes), so the
-  // subtree's slot range is emitted without descending.  A NaN in the window
-  // or the MBR fails the containment test and takes the normal path.
-  const bool contain = kContain && T.nlev > 0;
+  // A window that contains a node's MBR hits every ordinary box under it:
+  // x1 <= MBR.xmin <= xmin <= xmax <= MBR.xmax <= x2, and the same in y, so
+  // none of the predicate's four exclusions holds.  The subtree's slot range
+  // is then emitted without descending.  A box that is not ordinary (xmin >
+  // xmax, ymin > ymax, or a NaN coordinate, which the MBR's min/max skip) can
+  // fail the predicate under a contained MBR, so any such box in the set
+  // turns the shortcut off.  A NaN in the window or the MBR fails the
+  // containment test and takes the normal path.
+  const bool contain = kContain && T.nlev > 0 && (T.lvl_odd == nullptr || *T.lvl_odd == 0);
   // the root is never tested: its children range starts the frontier
   {
     int rp, rl;

@@ -146,6 +146,49 @@ def test_query_nan_window_follows_tree_semantics(crt):
     assert_all(all_forms(crt, d, rt, dq), want)
 
 
+def boxes_not_ordinary(n, seed):
+    """Uniform boxes, 600 of them made not ordinary: inverted in x, a ymax far
+    below the ymin, a NaN xmin or a NaN ymax."""
+    b = D.uniform_boxes(n, seed=seed)
+    k = np.random.default_rng(seed).choice(n, 600, replace=False)
+    inv, low, nx, ny = k[:200], k[200:400], k[400:500], k[500:]
+    b.xmin[inv], b.xmax[inv] = b.xmax[inv].copy(), b.xmin[inv].copy()
+    b.ymax[low] = b.ymin[low] - np.float32(0.02) * D.SCALE
+    b.xmin[nx] = np.nan
+    b.ymax[ny] = np.nan
+    return b
+
+
+@pytest.mark.parametrize("f", [4, 10, 16])
+def test_query_boxes_not_ordinary(crt, f):
+    """The predicate (src/rtree_bfs_frontier.cuh:40-44) can reject a box that
+    is not ordinary (xmin > xmax, ymin > ymax, or a NaN corner, which the
+    MBR's min/max skip) under a node whose MBR the window contains, so such a
+    box set must not take the containment shortcut: every form equals the
+    oracle's traversal, and the shortcut's test count equals the box-by-box
+    one."""
+    b = boxes_not_ordinary(80_000, seed=300 + f)
+    q = D.mixed_windows(1500, None, seed=400 + f, lo=1e-2, hi=0.5)
+    d, rt, dq, want = setup(crt, b, q, f)
+    assert len(want[0]) > 100_000
+    assert_all(all_forms(crt, d, rt, dq), want)
+    for nc in (0, 1):
+        got = canon(*crt.query(rt, d, dq, mode=crt.CRT_QUERY_PLAIN, no_contain=nc)[:2])
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), nc
+    s = crt.query_stats(rt, d, dq)
+    assert s["hits"] == len(want[0]) and s["tested_contain"] == s["tested"]
+    assert s["range_hits"] == 0
+    # the same boxes made ordinary again: the shortcut is back on
+    o = boxes_not_ordinary(80_000, seed=300 + f)
+    o.xmin, o.xmax = np.fmin(o.xmin, o.xmax), np.fmax(o.xmin, o.xmax)
+    o.ymin, o.ymax = np.fmin(o.ymin, o.ymax), np.fmax(o.ymin, o.ymax)
+    d2, rt2, dq2, want2 = setup(crt, o, q, f)
+    s2 = crt.query_stats(rt2, d2, dq2)
+    assert s2["hits"] == len(want2[0]) and s2["tested_contain"] < s2["tested"]
+    got = canon(*crt.query(rt2, d2, dq2))
+    assert np.array_equal(got[0], want2[0]) and np.array_equal(got[1], want2[1])
+
+
 @pytest.mark.parametrize("f", [2, 3, 10, 16, 32, 40])
 def test_large_windows_containment(crt, f):
     """Windows covering large parts of the domain: whole subtrees are emitted

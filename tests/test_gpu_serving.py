@@ -95,6 +95,33 @@ def test_results_same_alone_and_in_the_mix(env):
     assert srv.close() == 0
 
 
+def test_tree_with_boxes_not_ordinary(env):
+    """A served tree holding inverted boxes and NaN corners: the serving
+    kernel must not take the containment shortcut on it (the predicate can
+    reject such a box under a contained MBR); results equal the oracle's."""
+    C, Server, _ = env
+    b = D.uniform_boxes(200_000, seed=79)
+    k = np.random.default_rng(79).choice(b.n, 400, replace=False)
+    b.xmin[k[:200]], b.xmax[k[:200]] = b.xmax[k[:200]].copy(), b.xmin[k[:200]].copy()
+    b.ymax[k[200:]] = np.nan
+    d = C.BBox.from_host(b)
+    rt = C.RTree(10)
+    C.build_rtree(d, rt)
+    sb, t = O.build(b, 10)
+    tree = [{"rt": rt, "d": d, "sb": sb, "t": t, "f": 10}]
+    srv, ids = setup_server(C, Server, tree, arena_bytes=1 << 30)
+    reqs = [(0, D.mixed_windows(400, None, seed=790 + i, lo=1e-2, hi=0.5)) for i in range(4)]
+    done = run_all(srv, ids, reqs)
+    for i, (ti, w) in enumerate(reqs):
+        c, (fid, tid) = done[i]
+        assert c["status"] == 0
+        got = O.canonical_pairs(fid, tid)
+        want = expected(tree, ti, w)
+        assert len(want[0]) > 0
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), i
+    assert srv.close() == 0
+
+
 def test_overflow_and_retry(env):
     C, Server, trees = env
     srv, ids = setup_server(C, Server, trees, pairs_per_window=0.01, output_slack=0.01)
