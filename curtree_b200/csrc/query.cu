@@ -69,6 +69,10 @@ struct CountEmit {
   __device__ __forceinline__ void begin(int) {}
   __device__ __forceinline__ void operator()(bool hit, int) { hits += __popc(__ballot_sync(0xffffffffu, hit)); }
   __device__ __forceinline__ void range(const int*, long long, long long count) { hits += count; }
+  __device__ __forceinline__ void small_ranges(const int*, bool mine, long long, int count)
+  {
+    hits += __reduce_add_sync(0xffffffffu, mine ? (unsigned)count : 0u);
+  }
 };
 
 // Counts hits and the leaf boxes tested (workload statistics).
@@ -84,6 +88,12 @@ struct StatEmit {
   {
     hits += count;
     range_hits += count;
+  }
+  __device__ __forceinline__ void small_ranges(const int*, bool mine, long long, int count)
+  {
+    const unsigned n = __reduce_add_sync(0xffffffffu, mine ? (unsigned)count : 0u);
+    hits += n;
+    range_hits += n;
   }
 };
 
@@ -111,6 +121,10 @@ struct OffsetEmit {
   {
     copy_range(bid, first, count, fid, tid, base, cap, q);
     base += count;
+  }
+  __device__ __forceinline__ void small_ranges(const int* bid, bool mine, long long first, int count)
+  {
+    emit_small_ranges(*this, bid, mine, first, count);
   }
 };
 
@@ -225,6 +239,10 @@ struct ChunkEmit {
       __stcs(fid + slot, id);
       __stcs(tid + slot, q);
     }
+  }
+  __device__ __forceinline__ void small_ranges(const int* bid, bool mine, long long first, int count)
+  {
+    emit_small_ranges(*this, bid, mine, first, count);
   }
   // A contained subtree's ids are copied to an exact reservation of their
   // own (no unused chunk end); short ranges go through the chunk.

@@ -142,6 +142,10 @@ struct StagedEmit {
     __syncwarp();
   }
   __device__ __forceinline__ void begin(int qq) { q = qq; }
+  __device__ __forceinline__ void small_ranges(const int* bid, bool mine, long long first, int count)
+  {
+    emit_small_ranges(*this, bid, mine, first, count);
+  }
   // A contained subtree's ids go straight to an exact reservation.
   __device__ __forceinline__ void range(const int* bid, long long first, long long count)
   {

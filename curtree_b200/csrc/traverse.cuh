@@ -134,6 +134,44 @@ __device__ __forceinline__ void emit_range_default(Emit& emit, const int* __rest
   }
 }
 
+// Contained subtrees below this many boxes (a leaf-parent holds `fanout`)
+// are emitted together, all of one step's at once; larger ones one at a
+// time, each into an output reservation of its own.
+constexpr int kSmallRange = 256;
+
+// Emits the ids of every lane's slot range [first, first + count) (count <
+// kSmallRange; a lane with mine == false adds none), 32 ids per warp pass
+// whatever the ranges' sizes: each lane finds the range holding its id by a
+// binary search over the lanes' inclusive count prefix (warp-collective).
+template <class Emit>
+__device__ __forceinline__ void emit_small_ranges(Emit& emit, const int* __restrict__ bid, bool mine,
+                                                  long long first, int count)
+{
+  const int lane = (int)lane_id();
+  const int c = mine ? count : 0;
+  int x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  const int total = __shfl_sync(0xffffffffu, x, 31);
+  // element t of the concatenation, inside lane j's range, is id bid[base_j + t]
+  const long long base = first - (x - c);
+  for (int t0 = 0; t0 < total; t0 += 32) {
+    const int t = t0 + lane;
+    int j = 0;  // lanes whose inclusive prefix is <= t: the owner of t
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+      const int v = __shfl_sync(0xffffffffu, x, j + s - 1);
+      if (v <= t) j += s;
+    }
+    const long long b = __shfl_sync(0xffffffffu, base, j);
+    const bool ok = t < total;
+    emit(ok, ok ? __ldg(bid + b + t) : 0);
+  }
+}
+
 // Writes the pairs (bid[first + i], q) to output slots slot0 + i for
 // i < count, skipping slots at or past `cap` (warp-collective).  A contained
 // subtree can hold millions of boxes, so the ids are read as 16-byte vectors
@@ -308,7 +346,9 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
       }
       emit(hit, hid);
       if (contain) {
-        uint32_t im = __ballot_sync(0xffffffffu, inside);
+        const bool small = inside && rcount < kSmallRange;
+        if (__any_sync(0xffffffffu, small)) emit.small_ranges(T.bid, small, rfirst, (int)rcount);
+        uint32_t im = __ballot_sync(0xffffffffu, inside && !small);
         while (im) {
           const int src = __ffs(im) - 1;
           im &= im - 1;
