@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
   const long long q = (long long)blockIdx.x * kPlainWarps + warp;
   if (q >= W.n) return;
   int lg, lc;
-  lane_map(T.fanout, K, lg, lc);
+  lane_map(T.fanout, lg, lc);
   NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   CountEmit emit;
   traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
   if (q >= W.n) return;
   if (offsets[W.n] > cap) return;  // overflow: the host reports the required size
   int lg, lc;
-  lane_map(T.fanout, K, lg, lc);
+  lane_map(T.fanout, lg, lc);
   NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   OffsetEmit emit{fid, tid, offsets[q], cap, (int)q};
   traverse(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kPlainWarps * 32)
   const long long q = (long long)blockIdx.x * kPlainWarps + warp;
   if (q >= W.n) return;
   int lg, lc;
-  lane_map(T.fanout, K, lg, lc);
+  lane_map(T.fanout, lg, lc);
   NodeCache C{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   StatEmit emit;
   traverse<StatEmit, kContain>(T, C, K, lg, lc, W.xmin[q], W.ymin[q], W.xmax[q], W.ymax[q],
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks)
 
   FrontierEntry* stack = stacks + warp * P.stack_cap;
   int lg, lc;
-  lane_map(P.T.fanout, P.K, lg, lc);
+  lane_map(P.T.fanout, lg, lc);
   const uint32_t* order = nullptr;
   if (P.sort_ctrl) {
     const int na = P.sort_ctrl->n_active;

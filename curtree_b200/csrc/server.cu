@@ -103,6 +103,14 @@ struct SrvState {
   unsigned long long reserved;
 };
 
+// Control words in mapped (zero-copy) host memory: the host stops the loop
+// and reads its error status with plain loads and stores, no CUDA call, so
+// neither waits behind other work queued on the device.
+struct SrvCtl {
+  int shutdown;
+  int error;
+};
+
 constexpr int kSrvThreads = 256;
 constexpr int kSrvWarps = kSrvThreads / 32;
 constexpr int kStage = 256;  // staged pairs per warp
@@ -184,8 +192,8 @@ __device__ __forceinline__ void load_desc(const SrvDesc* p, SrvDesc& d)
 }
 
 __global__ void __launch_bounds__(kSrvThreads)
-    serve_kernel(SrvState* st, const SrvTree* __restrict__ trees, const SrvDesc* descs,
-                 SrvCtr* ctrs, SrvDone* done_host, int slots, int stack_cap,
+    serve_kernel(SrvState* st, SrvCtl* ctl, const SrvTree* __restrict__ trees,
+                 const SrvDesc* descs, SrvCtr* ctrs, SrvDone* done_host, int slots, int stack_cap,
                  unsigned long long wait_ns)
 {
   extern __shared__ int smem[];
@@ -206,6 +214,14 @@ __global__ void __launch_bounds__(kSrvThreads)
       unsigned sleep = 32;
       while (t >= ld_volatile_u64(&st->published)) {
         if (*(volatile int*)&st->shutdown) { state = 1; break; }
+        // one warp polls the host's mapped stop flag (a read across the
+        // host link) and relays it to the device word the others poll
+        if (blockIdx.x == 0 && warp == 0 && *(volatile int*)&ctl->shutdown) {
+          *(volatile int*)&st->shutdown = 1;
+          __threadfence();
+          state = 1;
+          break;
+        }
         unsigned long long now;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
         if (now - t0 > wait_ns) { state = 2; break; }
@@ -245,7 +261,7 @@ __global__ void __launch_bounds__(kSrvThreads)
     T.nlev = tr.nlev; T.lvl_first = tr.lvl_first; T.lvl_span = tr.lvl_span;
     T.lvl_odd = tr.lvl_odd;
     int lg, lc;
-    lane_map(T.fanout, tr.K, lg, lc);
+    lane_map(T.fanout, lg, lc);
     SrvCtr* ctr = &ctrs[r % slots];
     StagedEmit emit;
     emit.s_fid = stage;
@@ -272,6 +288,14 @@ __global__ void __launch_bounds__(kSrvThreads)
       }
     }
     __syncwarp();
+  }
+  // a warp that leaves on an error reports it to the host's mapped word
+  if (lane == 0) {
+    const int e = *(volatile int*)&st->error;
+    if (e) {
+      *(volatile int*)&ctl->error = e;
+      __threadfence_system();
+    }
   }
 }
 
@@ -378,6 +402,24 @@ struct Server {
   SrvDone* h_done = nullptr;  // pinned, mapped
   SrvDone* d_done = nullptr;
   SrvDesc* h_desc_stage = nullptr;  // pinned staging for descriptor uploads
+  // Copies made while the device loop may run go through pinned host memory
+  // (asynchronous on their stream; a pageable copy is staged by the host
+  // thread and returns only when it is done).  The loop's stop flag and error
+  // status are mapped words (SrvCtl) that need no copy at all: a copy can
+  // still wait behind other work queued on the device, such as a client's
+  // kernel waiting for SM slots the loop holds.
+  struct Mailbox {
+    SrvState launch;
+    unsigned long long published;
+  };
+  Mailbox* h_box = nullptr;             // pinned: the dispatcher's words
+  SrvCtl* h_ctl = nullptr;              // mapped: stop flag and error status
+  SrvCtl* d_ctl = nullptr;
+  static constexpr size_t kBounce = 8u << 20;
+  char* h_bounce = nullptr;             // pinned bounce buffer: the dispatcher
+  char* h_bounce_submit = nullptr;      // pinned bounce buffer: submitters
+  std::mutex submit_mu;                 // guards h_bounce_submit and `upload`
+  cudaStream_t upload = nullptr;        // submitters' window copies
   int slots = 0;
   int stack_cap = 32;
   // bookkeeping
@@ -403,26 +445,65 @@ struct Server {
   {
     return (size_t)kSrvWarps * stack_cap * sizeof(FrontierEntry) + (size_t)kSrvWarps * 2 * kStage * 4;
   }
+  // All CTA slots but one SM's worth: a loop that held every slot would keep
+  // any other kernel of the process (a client's, a library's) from starting
+  // until it stops, and work queued behind that kernel -- copies included --
+  // would wait too.  The block scheduler spreads the CTAs, so a few SMs keep
+  // a free slot.
   int grid() const
   {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kSrvThreads, smem());
-    return std::max(1, per_sm) * sm_count();
+    per_sm = std::max(1, per_sm);
+    return std::max(1, per_sm * sm_count() - per_sm);
+  }
+
+  // Copies `bytes` between pageable host memory and the device in kBounce
+  // pieces through the pinned buffer `buf`, on stream `st`.
+  static cudaError_t bounce_copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind,
+                                 char* buf, cudaStream_t st)
+  {
+    for (size_t off = 0; off < bytes; off += kBounce) {
+      const size_t n = std::min(kBounce, bytes - off);
+      cudaError_t e;
+      if (kind == cudaMemcpyHostToDevice) {
+        std::memcpy(buf, (const char*)src + off, n);
+        e = cudaMemcpyAsync((char*)dst + off, buf, n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      } else {
+        e = cudaMemcpyAsync(buf, (const char*)src + off, n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) std::memcpy((char*)dst + off, buf, n);
+      }
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+
+  // The device loop's last error status (the mapped word).
+  int read_device_error()
+  {
+    std::atomic_thread_fence(std::memory_order_acquire);
+    return *(volatile int*)&h_ctl->error;
   }
 
   void launch_kernel()
   {
     // reset the ticket counter to the published count: tickets taken past it
     // by the previous instance carried no work
-    SrvState s{};
+    SrvState& s = h_box->launch;
+    s = SrvState{};
     s.next_ticket = published;
     s.published = published;
     s.r_start = oldest_seq;
     cudaMemcpyAsync(d_state, &s, sizeof(s), cudaMemcpyHostToDevice, copy);
     cudaStreamSynchronize(copy);
+    *(volatile int*)&h_ctl->shutdown = 0;
+    *(volatile int*)&h_ctl->error = 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
     cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
     serve_kernel<<<grid(), kSrvThreads, smem(), compute>>>(
-        d_state, d_trees, d_descs, d_ctrs, d_done, slots, stack_cap,
+        d_state, d_ctl, d_trees, d_descs, d_ctrs, d_done, slots, stack_cap,
         (unsigned long long)opts.device_wait_us * 1000ull);
     CRT_LAUNCHED(1);
     kernel_running = true;
@@ -430,12 +511,10 @@ struct Server {
 
   void stop_kernel()
   {
-    int one = 1;
-    cudaMemcpyAsync(&d_state->shutdown, &one, sizeof(int), cudaMemcpyHostToDevice, copy);
-    cudaStreamSynchronize(copy);
+    *(volatile int*)&h_ctl->shutdown = 1;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
     cudaStreamSynchronize(compute);
-    int err = 0;
-    cudaMemcpy(&err, &d_state->error, sizeof(int), cudaMemcpyDeviceToHost);
+    const int err = read_device_error();
     if (err) device_error = err;
     kernel_running = false;
   }
@@ -471,8 +550,9 @@ struct Server {
       flight.emplace(q.seq, q);
     }
     cudaStreamSynchronize(copy);  // descriptors and counters are in device memory
-    cudaMemcpyAsync(&d_state->published, &published, sizeof(published), cudaMemcpyHostToDevice,
-                    copy);
+    h_box->published = published;
+    cudaMemcpyAsync(&d_state->published, &h_box->published, sizeof(published),
+                    cudaMemcpyHostToDevice, copy);
     cudaStreamSynchronize(copy);
   }
 
@@ -544,9 +624,8 @@ struct Server {
             n_retried++;
             Request rq = q;
             rq.host_windows = std::make_shared<std::vector<float>>((size_t)q.nq * 4);
-            cudaError_t ce = cudaMemcpyAsync(rq.host_windows->data(), arena + q.win_off,
-                                             (size_t)q.nq * 16, cudaMemcpyDeviceToHost, copy);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(copy);
+            cudaError_t ce = bounce_copy(rq.host_windows->data(), arena + q.win_off,
+                                         (size_t)q.nq * 16, cudaMemcpyDeviceToHost, h_bounce, copy);
             alloc.release(q.out_off, q.out_bytes);
             alloc.release(q.win_off, q.win_bytes);
             rq.cap = count;
@@ -589,9 +668,8 @@ struct Server {
         retry_wait.pop_front();
         rq.win_off = off;
         rq.out_off = off + granules(rq.win_bytes);
-        cudaError_t ce = cudaMemcpyAsync(arena + rq.win_off, rq.host_windows->data(),
-                                         (size_t)rq.nq * 16, cudaMemcpyHostToDevice, copy);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(copy);
+        cudaError_t ce = bounce_copy(arena + rq.win_off, rq.host_windows->data(),
+                                     (size_t)rq.nq * 16, cudaMemcpyHostToDevice, h_bounce, copy);
         rq.host_windows.reset();
         if (ce != cudaSuccess) {
           cudaGetLastError();
@@ -618,10 +696,8 @@ struct Server {
       }
       if (kernel_running && now_s() - last_err_check > 1e-3) {
         last_err_check = now_s();
-        int err = 0;
         // a timed-out device loop: report it on every request in flight
-        cudaMemcpyAsync(&err, &d_state->error, sizeof(int), cudaMemcpyDeviceToHost, copy);
-        cudaStreamSynchronize(copy);
+        const int err = read_device_error();
         if (err) {
           // some warps gave up waiting (the host stalled past device_wait_us)
           // and may have dropped tickets: stop the loop, then re-run every
@@ -708,6 +784,20 @@ int crt_server_create(const crt_server_opts* opts, crt_server* out)
     if ((e = cudaHostAlloc((void**)&s->h_desc_stage, sizeof(SrvDesc) * s->slots,
                            cudaHostAllocDefault)) != cudaSuccess)
       break;
+    if ((e = cudaHostAlloc((void**)&s->h_box, sizeof(Server::Mailbox), cudaHostAllocDefault)) !=
+        cudaSuccess)
+      break;
+    if ((e = cudaHostAlloc((void**)&s->h_ctl, sizeof(SrvCtl), cudaHostAllocMapped)) != cudaSuccess)
+      break;
+    if ((e = cudaHostGetDevicePointer((void**)&s->d_ctl, s->h_ctl, 0)) != cudaSuccess) break;
+    s->h_ctl->shutdown = 0;
+    s->h_ctl->error = 0;
+    if ((e = cudaHostAlloc((void**)&s->h_bounce, Server::kBounce, cudaHostAllocDefault)) != cudaSuccess)
+      break;
+    if ((e = cudaHostAlloc((void**)&s->h_bounce_submit, Server::kBounce, cudaHostAllocDefault)) !=
+        cudaSuccess)
+      break;
+    if ((e = cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking)) != cudaSuccess) break;
   } while (0);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -815,6 +905,7 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
   if (!s || nq < 1 || !xmin || !ymin || !xmax || !ymax)
     return fail(CRT_ERR_INVALID_ARG, "server_submit: bad arguments");
   Request q;
+  bool pageable = false;  // the windows are in pageable host memory
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (tree_id < 0 || tree_id >= (int)s->trees.size())
@@ -833,6 +924,7 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
     const bool host_windows = cudaPointerGetAttributes(&pa, xmin) == cudaSuccess &&
                               pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged;
     cudaGetLastError();
+    pageable = host_windows && pa.type == cudaMemoryTypeUnregistered;
     if (host_windows) {
       q.predicted = s->predict_locked(tree_id, xmin, ymin, xmax, ymax, nq);
     } else {
@@ -842,9 +934,12 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
       std::vector<float> hw((size_t)nq * 4);
       const float* src[4] = {xmin, ymin, xmax, ymax};
       cudaError_t ce = cudaSuccess;
-      for (int a = 0; a < 4 && ce == cudaSuccess; a++)
-        ce = cudaMemcpy(hw.data() + (size_t)a * nq, src[a], sizeof(float) * (size_t)nq,
-                        cudaMemcpyDeviceToHost);
+      {
+        std::lock_guard<std::mutex> ul(s->submit_mu);
+        for (int a = 0; a < 4 && ce == cudaSuccess; a++)
+          ce = Server::bounce_copy(hw.data() + (size_t)a * nq, src[a], sizeof(float) * (size_t)nq,
+                                   cudaMemcpyDeviceToHost, s->h_bounce_submit, s->upload);
+      }
       if (ce == cudaSuccess)
         q.predicted = s->predict_locked(tree_id, hw.data(), hw.data() + nq, hw.data() + 2 * nq,
                                         hw.data() + 3 * nq, nq);
@@ -871,9 +966,15 @@ int crt_server_submit(crt_server h, int tree_id, const float* xmin, const float*
   float* w = (float*)(s->arena + q.win_off);
   cudaError_t e = cudaSuccess;
   const float* src[4] = {xmin, ymin, xmax, ymax};
-  for (int a = 0; a < 4 && e == cudaSuccess; a++)
-    e = cudaMemcpyAsync(w + a * nq, src[a], sizeof(float) * (size_t)nq, cudaMemcpyDefault, s->copy);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->copy);
+  {
+    std::lock_guard<std::mutex> ul(s->submit_mu);
+    for (int a = 0; a < 4 && e == cudaSuccess; a++)
+      e = pageable ? Server::bounce_copy(w + a * nq, src[a], sizeof(float) * (size_t)nq,
+                                         cudaMemcpyHostToDevice, s->h_bounce_submit, s->upload)
+                   : cudaMemcpyAsync(w + a * nq, src[a], sizeof(float) * (size_t)nq,
+                                     cudaMemcpyDefault, s->upload);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload);
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (e != cudaSuccess) {
     s->alloc.release(q.win_off, q.win_bytes);
@@ -949,6 +1050,11 @@ int crt_server_destroy(crt_server h)
   cudaFree(s->d_state);
   if (s->h_done) cudaFreeHost(s->h_done);
   if (s->h_desc_stage) cudaFreeHost(s->h_desc_stage);
+  if (s->h_box) cudaFreeHost(s->h_box);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_bounce) cudaFreeHost(s->h_bounce);
+  if (s->h_bounce_submit) cudaFreeHost(s->h_bounce_submit);
+  if (s->upload) cudaStreamDestroy(s->upload);
   if (s->compute) cudaStreamDestroy(s->compute);
   if (s->copy) cudaStreamDestroy(s->copy);
   const int err = s->device_error;

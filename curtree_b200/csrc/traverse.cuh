@@ -172,14 +172,6 @@ __device__ __forceinline__ void emit_small_ranges(Emit& emit, const int* __restr
   }
 }
 
-// Writes the pairs (bid[first + i], q) to output slots slot0 + i for
-// i < count, skipping slots at or past `cap` (warp-collective).  A contained
-// subtree can hold millions of boxes, so the ids are read as 16-byte vectors
-// (128 ids per warp step, kRangeUnroll steps in flight) instead of one 4-byte
-// load per lane; one step keeps the persistent kernels within their register
-// budgets.
-constexpr int kRangeUnroll = 1;
-
 // Pair stores use the evict-first hint (st.global.cs): the output streams
 // through L2 once, and keeping it out of the way leaves L2 to the tree's
 // boxes and ids (measured: 1-3% on the uniform batch, 7-10% on road
@@ -193,48 +185,142 @@ __device__ __forceinline__ void put_pair(int32_t* __restrict__ fid, int32_t* __r
   }
 }
 
+// Four pairs at output slot sl (16-byte aligned in fid and tid), or one by
+// one where they reach cap.
+__device__ __forceinline__ void put_pairs4(int32_t* __restrict__ fid, int32_t* __restrict__ tid,
+                                           long long sl, long long cap, int4 v, int q)
+{
+  if (sl + 3 < cap) {
+    __stcs(reinterpret_cast<int4*>(fid + sl), v);
+    if (tid) __stcs(reinterpret_cast<int4*>(tid + sl), make_int4(q, q, q, q));
+  } else {
+    put_pair(fid, tid, sl + 0, cap, v.x, q);
+    put_pair(fid, tid, sl + 1, cap, v.y, q);
+    put_pair(fid, tid, sl + 2, cap, v.z, q);
+    put_pair(fid, tid, sl + 3, cap, v.w, q);
+  }
+}
+
+// Writes the pairs (bid[first + i], q) to output slots slot0 + i for
+// i < count, skipping slots at or past `cap` (warp-collective).  A contained
+// subtree can hold millions of boxes, so ids move 128 per warp pass as
+// 16-byte vectors: the output is aligned first (up to 3 ids one by one);
+// when the source then sits at another offset within its 16 bytes, each
+// lane's four ids come from its own aligned source vector and its
+// neighbour's (one shuffle per component), so loads and stores both stay
+// 16-byte accesses wherever the reservation starts.  Only aligned vectors
+// inside [bid, bid + first + count) are read.
 __device__ __forceinline__ void copy_range(const int* __restrict__ bid, long long first,
                                            long long count, int32_t* __restrict__ fid,
                                            int32_t* __restrict__ tid, long long slot0,
                                            long long cap, int q)
 {
   const int lane = (int)lane_id();
-  const int* src = bid + first;
-  // head: ids before the first 16-byte boundary of the source
-  long long head = (long long)((4 - (((uintptr_t)src >> 2) & 3)) & 3);
+  if (count <= 0) return;
+  const uintptr_t fa = (uintptr_t)(fid + slot0);
+  // vectors need bid 16-byte aligned and fid, tid at one offset within 16 bytes
+  const bool vec = ((uintptr_t)bid & 15) == 0 &&
+                   (!tid || (((uintptr_t)(tid + slot0) ^ fa) & 15) == 0);
+  if (!vec) {
+    for (long long i = lane; i < count; i += 32)
+      put_pair(fid, tid, slot0 + i, cap, __ldg(bid + first + i), q);
+    return;
+  }
+  // head: ids before the output's first 16-byte boundary
+  long long head = (long long)((4 - ((fa >> 2) & 3)) & 3);
   if (head > count) head = count;
-  if (lane < head) put_pair(fid, tid, slot0 + lane, cap, __ldg(src + lane), q);
-  const int4* v = reinterpret_cast<const int4*>(src + head);
-  const long long nv = (count - head) >> 2;
-  const long long s = slot0 + head;
-  for (long long g0 = 0; g0 < nv; g0 += 32 * kRangeUnroll) {
-    int4 r[kRangeUnroll];
-#pragma unroll
-    for (int u = 0; u < kRangeUnroll; u++) {
-      const long long g = g0 + u * 32 + lane;
-      if (g < nv) r[u] = __ldg(v + g);
-    }
-#pragma unroll
-    for (int u = 0; u < kRangeUnroll; u++) {
-      const long long g = g0 + u * 32 + lane;
-      if (g < nv) {
-        const long long sl = s + 4 * g;
-        const uintptr_t al = (uintptr_t)(fid + sl) | (tid ? (uintptr_t)(tid + sl) : (uintptr_t)0);
-        if (sl + 3 < cap && (al & 15) == 0) {
-          __stcs(reinterpret_cast<int4*>(fid + sl), r[u]);
-          if (tid) __stcs(reinterpret_cast<int4*>(tid + sl), make_int4(q, q, q, q));
-        } else {
-          put_pair(fid, tid, sl + 0, cap, r[u].x, q);
-          put_pair(fid, tid, sl + 1, cap, r[u].y, q);
-          put_pair(fid, tid, sl + 2, cap, r[u].z, q);
-          put_pair(fid, tid, sl + 3, cap, r[u].w, q);
-        }
+  if (lane < head) put_pair(fid, tid, slot0 + lane, cap, __ldg(bid + first + lane), q);
+  const long long f1 = first + head;  // first source id of the body
+  const long long s1 = slot0 + head;  // its output slot, 16-byte aligned
+  const long long end = first + count;
+  const int r = (int)(f1 & 3);  // source offset within its 16 bytes
+  const long long B = f1 - r;   // the aligned source vector holding f1
+  const int4* __restrict__ v = reinterpret_cast<const int4*>(bid + B);
+  long long ng;  // output vectors of the body
+  if (r == 0) {
+    ng = (end - f1) >> 2;
+    for (long long g = lane; g < ng; g += 32) put_pairs4(fid, tid, s1 + 4 * g, cap, __ldg(v + g), q);
+  } else {
+    // output vector g takes source vectors g and g + 1, both inside [B, end)
+    // for g < ng
+    ng = end - B >= 8 ? ((end - B - 8) >> 2) + 1 : 0;
+    for (long long g0 = 0; g0 < ng; g0 += 32) {
+      const long long g = g0 + lane;
+      int4 x = make_int4(0, 0, 0, 0);
+      if (g <= ng) x = __ldg(v + g);
+      int4 n;
+      n.x = __shfl_down_sync(0xffffffffu, x.x, 1);
+      n.y = __shfl_down_sync(0xffffffffu, x.y, 1);
+      n.z = __shfl_down_sync(0xffffffffu, x.z, 1);
+      n.w = __shfl_down_sync(0xffffffffu, x.w, 1);
+      if (lane == 31 && g + 1 <= ng) n = __ldg(v + g + 1);
+      if (g < ng) {
+        int4 o;
+        if (r == 1) o = make_int4(x.y, x.z, x.w, n.x);
+        else if (r == 2) o = make_int4(x.z, x.w, n.x, n.y);
+        else o = make_int4(x.w, n.x, n.y, n.z);
+        put_pairs4(fid, tid, s1 + 4 * g, cap, o, q);
       }
     }
   }
-  // tail: the last (count - head) % 4 ids
-  const long long done = head + 4 * nv;
-  if (lane < count - done) put_pair(fid, tid, slot0 + done + lane, cap, __ldg(src + done + lane), q);
+  // tail: the ids past the body (fewer than 8)
+  for (long long i = f1 + 4 * ng + lane; i < end; i += 32)
+    put_pair(fid, tid, s1 + (i - f1), cap, __ldg(bid + i), q);
+}
+
+// Outcome of testing one child slot of a step.
+struct ChildTest {
+  bool valid, hit, push, inside;
+  int hid, cpos, clen;
+  long long rfirst, rcount;
+  bool leaf;  // a box slot (counted as a leaf test)
+};
+
+// Tests child c of popped entry g (of k popped; lane e of the warp holds
+// entry e): a leaf box against the window, or an inner node (intersects:
+// push its children range; contained: emit its boxes' slot range).
+__device__ __forceinline__ void test_child(const TreeView& T, const NodeCache& C, FrontierEntry e,
+                                           int k, int g, int c, bool contain, float x1, float y1,
+                                           float x2, float y2, ChildTest& t)
+{
+  const int gs = min(g, k - 1);
+  const int pos = __shfl_sync(0xffffffffu, e.x, gs);
+  const int ey = __shfl_sync(0xffffffffu, e.y, gs);
+  const int len = contain ? (ey & kLenMask) : ey;
+  const int hc = contain ? (ey >> kLenBits) : 0;  // height of the nodes [pos, pos+len)
+  t.valid = g < k && c < len;
+  const int child = pos + c;
+  t.hit = t.push = t.inside = t.leaf = false;
+  t.hid = t.cpos = t.clen = 0;
+  t.rfirst = t.rcount = 0;
+  if (!t.valid) return;
+  if (pos >= T.rsz) {
+    const int s = child - T.rsz;
+    if (s < T.nbox) {
+      t.leaf = true;
+      // the id is loaded with the box (one round trip; most tested boxes of
+      // a leaf-parent that straddles the window hit)
+      const float m1 = __ldg(T.bxmin + s), n1 = __ldg(T.bymin + s);
+      const float m2 = __ldg(T.bxmax + s), n2 = __ldg(T.bymax + s);
+      const int id = __ldg(T.bid + s);
+      t.hit = intersects(x1, y1, x2, y2, m1, n1, m2, n2);
+      t.hid = id;
+    }
+  } else if (child < T.rsz) {
+    float a, b, cc, d;
+    load_node_box(T, C, child, a, b, cc, d);
+    load_node_link(T, C, child, t.cpos, t.clen);
+    t.push = intersects(x1, y1, x2, y2, a, b, cc, d);
+    if (contain && t.push && x1 <= a && cc <= x2 && y1 <= b && d <= y2) {
+      t.inside = true;
+      t.push = false;
+      const long long span = __ldg(T.lvl_span + hc);
+      t.rfirst = (long long)(child - __ldg(T.lvl_first + hc)) * span;
+      t.rcount = min((long long)T.nbox - t.rfirst, span);
+    } else if (contain) {
+      t.clen |= max(hc - 1, 0) << kLenBits;
+    }
+  }
 }
 
 // part / nparts: this warp takes the part-th of nparts equal shares of the
@@ -294,46 +380,11 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
     __syncwarp();
     const int span = f <= 32 ? 32 : f;  // children covered per node group
     for (int base = 0; base < span; base += 32) {
-      int g, c;
-      if (f <= 32) { g = lane_g; c = lane_c; }
-      else { g = 0; c = base + lane; }
-      const int gs = min(g, k - 1);
-      const int pos = __shfl_sync(0xffffffffu, e.x, gs);
-      const int ey = __shfl_sync(0xffffffffu, e.y, gs);
-      const int len = contain ? (ey & kLenMask) : ey;
-      const int hc = contain ? (ey >> kLenBits) : 0;  // height of the nodes [pos, pos+len)
-      const bool valid = g < k && c < len;
-      const int child = pos + c;
-      bool hit = false, push = false, inside = false;
-      int hid = 0, cpos = 0, clen = 0;
-      long long rfirst = 0, rcount = 0;
-      if (valid) {
-        if (pos >= T.rsz) {
-          const int s = child - T.rsz;
-          if (s < T.nbox) {
-            hit = intersects(x1, y1, x2, y2, __ldg(T.bxmin + s), __ldg(T.bymin + s),
-                             __ldg(T.bxmax + s), __ldg(T.bymax + s));
-            if (hit) hid = __ldg(T.bid + s);
-          }
-        } else if (child < T.rsz) {
-          float a, b, cc, d;
-          load_node_box(T, C, child, a, b, cc, d);
-          load_node_link(T, C, child, cpos, clen);
-          push = intersects(x1, y1, x2, y2, a, b, cc, d);
-          if (contain && push && x1 <= a && cc <= x2 && y1 <= b && d <= y2) {
-            inside = true;
-            push = false;
-            const long long span = __ldg(T.lvl_span + hc);
-            rfirst = (long long)(child - __ldg(T.lvl_first + hc)) * span;
-            rcount = min((long long)T.nbox - rfirst, span);
-          } else if (contain) {
-            clen |= max(hc - 1, 0) << kLenBits;
-          }
-        }
-      }
-      if constexpr (Emit::kCountsTests)
-        emit.leaf_tests(__popc(__ballot_sync(0xffffffffu, valid && pos >= T.rsz && child - T.rsz < T.nbox)));
-      const uint32_t pm = __ballot_sync(0xffffffffu, push);
+      ChildTest t;
+      if (f <= 32) test_child(T, C, e, k, lane_g, lane_c, contain, x1, y1, x2, y2, t);
+      else test_child(T, C, e, k, 0, base + lane, contain, x1, y1, x2, y2, t);
+      if constexpr (Emit::kCountsTests) emit.leaf_tests(__popc(__ballot_sync(0xffffffffu, t.leaf)));
+      const uint32_t pm = __ballot_sync(0xffffffffu, t.push);
       if (pm) {
         const int np = __popc(pm);
         if (sp + np > stack_cap) {
@@ -341,19 +392,19 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
           raise_error(err, CRT_ERR_NOT_SUPPORTED);
           return;
         }
-        if (push) stack[sp + __popc(pm & lt)] = make_int2(cpos, clen);
+        if (t.push) stack[sp + __popc(pm & lt)] = make_int2(t.cpos, t.clen);
         sp += np;
       }
-      emit(hit, hid);
+      emit(t.hit, t.hid);
       if (contain) {
-        const bool small = inside && rcount < kSmallRange;
-        if (__any_sync(0xffffffffu, small)) emit.small_ranges(T.bid, small, rfirst, (int)rcount);
-        uint32_t im = __ballot_sync(0xffffffffu, inside && !small);
+        const bool small = t.inside && t.rcount < kSmallRange;
+        if (__any_sync(0xffffffffu, small)) emit.small_ranges(T.bid, small, t.rfirst, (int)t.rcount);
+        uint32_t im = __ballot_sync(0xffffffffu, t.inside && !small);
         while (im) {
           const int src = __ffs(im) - 1;
           im &= im - 1;
-          emit.range(T.bid, __shfl_sync(0xffffffffu, rfirst, src),
-                     __shfl_sync(0xffffffffu, rcount, src));
+          emit.range(T.bid, __shfl_sync(0xffffffffu, t.rfirst, src),
+                     __shfl_sync(0xffffffffu, t.rcount, src));
         }
       }
     }
@@ -361,14 +412,15 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
   }
 }
 
-// Lane -> (node group, child) for fanout <= 32.
-__device__ __forceinline__ void lane_map(int f, int K, int& g, int& c)
+// Lane -> (node group, child) of its first child slot, for fanout <= 32;
+// lanes past the last whole group get group 32 (never valid).
+__device__ __forceinline__ void lane_map(int f, int& g, int& c)
 {
   const int lane = (int)lane_id();
   if (f <= 32) {
     g = lane / f;
     c = lane - g * f;
-    if (g >= K) { g = 32; c = 0; }
+    if (g >= 32 / f) { g = 32; c = 0; }
   } else {
     g = 0;
     c = lane;

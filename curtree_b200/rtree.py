@@ -39,24 +39,32 @@ def _stream_handle(stream=None):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
+class _DeviceBytes:
+    """A raw device byte range, seen by torch through the CUDA array
+    interface (no copy)."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (int(nbytes),), "typestr": "|u1",
+                                         "data": (int(ptr), False), "version": 2}
+
+
+def _device_bytes(ptr: int, nbytes: int):
+    return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
+
+
 def _d2h(ptr: int, n: int, dtype) -> np.ndarray:
     """Copy n elements at a device address into a new numpy array."""
     out = np.empty(n, dtype)
     if n:
-        t = torch.empty(n * out.itemsize, dtype=torch.uint8, device="cuda")
-        _copy_ptr(t.data_ptr(), ptr, n * out.itemsize)
-        out[:] = t.cpu().numpy().view(dtype)
+        out[:] = _device_bytes(ptr, n * out.itemsize).cpu().numpy().view(dtype)
     return out
 
 
 def _copy_ptr(dst: int, src: int, nbytes: int) -> None:
     """Device-to-device copy between raw addresses on the current stream."""
-    from cuda.bindings import runtime as rt
-    err, = rt.cudaMemcpyAsync(dst, src, nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice,
-                              torch.cuda.current_stream().cuda_stream)
-    if int(err) != 0:
-        raise RuntimeError(f"cudaMemcpyAsync failed: {err}")
-    torch.cuda.current_stream().synchronize()
+    if nbytes:
+        _device_bytes(dst, nbytes).copy_(_device_bytes(src, nbytes))
+        torch.cuda.current_stream().synchronize()
 
 
 class BBox:
