@@ -73,6 +73,10 @@ struct CountEmit {
   {
     hits += __reduce_add_sync(0xffffffffu, mine ? (unsigned)count : 0u);
   }
+  __device__ __forceinline__ void big_ranges(const int* bid, bool mine, long long first, long long count)
+  {
+    emit_ranges_each(*this, bid, mine, first, count);
+  }
 };
 
 // Counts hits and the leaf boxes tested (workload statistics).
@@ -94,6 +98,10 @@ struct StatEmit {
     const unsigned n = __reduce_add_sync(0xffffffffu, mine ? (unsigned)count : 0u);
     hits += n;
     range_hits += n;
+  }
+  __device__ __forceinline__ void big_ranges(const int* bid, bool mine, long long first, long long count)
+  {
+    emit_ranges_each(*this, bid, mine, first, count);
   }
 };
 
@@ -125,6 +133,10 @@ struct OffsetEmit {
   __device__ __forceinline__ void small_ranges(const int* bid, bool mine, long long first, int count)
   {
     emit_small_ranges(*this, bid, mine, first, count);
+  }
+  __device__ __forceinline__ void big_ranges(const int* bid, bool mine, long long first, long long count)
+  {
+    emit_ranges_each(*this, bid, mine, first, count);
   }
 };
 
@@ -244,20 +256,43 @@ struct ChunkEmit {
   {
     emit_small_ranges(*this, bid, mine, first, count);
   }
-  // A contained subtree's ids are copied to an exact reservation of their
-  // own (no unused chunk end); short ranges go through the chunk.
-  __device__ __forceinline__ void range(const int* bid, long long first, long long count)
+  // Large contained subtrees go to an exact reservation (no unused chunk
+  // end), all of one step's in one: each lane's range at its prefix offset.
+  // One atomic per step instead of one per range keeps the shared output
+  // counter from becoming the bottleneck when every warp meets large
+  // subtrees at once (10M boxes x 250k windows of side 1e-2..1e-1: 21 ms
+  // with one atomic per range, 12.4 ms with one per step).
+  __device__ __forceinline__ void big_ranges(const int* bid, bool mine, long long first, long long count)
   {
-    if (count < 256) {
-      emit_range_default(*this, bid, first, count);
-      return;
+    const int lane = (int)lane_id();
+    const long long c = mine ? count : 0;
+    long long x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
+    const long long total = __shfl_sync(0xffffffffu, x, 31);
     unsigned long long nb = 0;
-    if (lane_id() == 0) nb = atomicAdd(next, (unsigned long long)count);
+    if (lane == 0) nb = atomicAdd(next, (unsigned long long)total);
     nb = __shfl_sync(0xffffffffu, nb, 0);
+    const long long excl = x - c;
+    uint32_t im = __ballot_sync(0xffffffffu, mine);
+    while (im) {
+      const int src = __ffs(im) - 1;
+      im &= im - 1;
+      place(bid, __shfl_sync(0xffffffffu, first, src), __shfl_sync(0xffffffffu, count, src),
+            (long long)nb + __shfl_sync(0xffffffffu, excl, src));
+    }
+  }
+  // Copies a contained subtree's ids to its reservation at output slot nb
+  // (large ones cut into pieces that idle warps copy).
+  __device__ __forceinline__ void place(const int* bid, long long first, long long count,
+                                        long long nb)
+  {
     hits += count;
     if (!jobs || count < kShareMin) {
-      copy_range(bid, first, count, fid, tid, (long long)nb, cap, q);
+      copy_range(bid, first, count, fid, tid, nb, cap, q);
       return;
     }
     // publish the pieces; the ones the queue has no room for are copied here

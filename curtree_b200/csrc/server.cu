@@ -154,6 +154,10 @@ struct StagedEmit {
   {
     emit_small_ranges(*this, bid, mine, first, count);
   }
+  __device__ __forceinline__ void big_ranges(const int* bid, bool mine, long long first, long long count)
+  {
+    emit_ranges_each(*this, bid, mine, first, count);
+  }
   // A contained subtree's ids go straight to an exact reservation.
   __device__ __forceinline__ void range(const int* bid, long long first, long long count)
   {

@@ -134,6 +134,20 @@ __device__ __forceinline__ void emit_range_default(Emit& emit, const int* __rest
   }
 }
 
+// Emits every lane's slot range one after the other through emit.range
+// (warp-collective).
+template <class Emit>
+__device__ __forceinline__ void emit_ranges_each(Emit& emit, const int* __restrict__ bid, bool mine,
+                                                 long long first, long long count)
+{
+  uint32_t im = __ballot_sync(0xffffffffu, mine);
+  while (im) {
+    const int src = __ffs(im) - 1;
+    im &= im - 1;
+    emit.range(bid, __shfl_sync(0xffffffffu, first, src), __shfl_sync(0xffffffffu, count, src));
+  }
+}
+
 // Contained subtrees below this many boxes (a leaf-parent holds `fanout`)
 // are emitted together, all of one step's at once; larger ones one at a
 // time, each into an output reservation of its own.
@@ -399,13 +413,8 @@ __device__ __forceinline__ void traverse(const TreeView& T, const NodeCache& C, 
       if (contain) {
         const bool small = t.inside && t.rcount < kSmallRange;
         if (__any_sync(0xffffffffu, small)) emit.small_ranges(T.bid, small, t.rfirst, (int)t.rcount);
-        uint32_t im = __ballot_sync(0xffffffffu, t.inside && !small);
-        while (im) {
-          const int src = __ffs(im) - 1;
-          im &= im - 1;
-          emit.range(T.bid, __shfl_sync(0xffffffffu, t.rfirst, src),
-                     __shfl_sync(0xffffffffu, t.rcount, src));
-        }
+        const bool big = t.inside && !small;
+        if (__any_sync(0xffffffffu, big)) emit.big_ranges(T.bid, big, t.rfirst, t.rcount);
       }
     }
     __syncwarp();
