@@ -292,7 +292,7 @@ struct ChunkEmit {
   {
     hits += count;
     if (!jobs || count < kShareMin) {
-      copy_range(bid, first, count, fid, tid, nb, cap, q);
+      copy_range_realign(bid, first, count, fid, tid, nb, cap, q);
       return;
     }
     // publish the pieces; the ones the queue has no room for are copied here

@@ -195,7 +195,9 @@ __device__ __forceinline__ void load_desc(const SrvDesc* p, SrvDesc& d)
   for (int i = 0; i < (int)(sizeof(SrvDesc) / 8); i++) dst[i] = __ldcg(src + i);
 }
 
-__global__ void __launch_bounds__(kSrvThreads)
+// Three CTAs per SM (at most 85 registers): at two the loop has a third
+// fewer warps to hide the traversal's memory latency with.
+__global__ void __launch_bounds__(kSrvThreads, 3)
     serve_kernel(SrvState* st, SrvCtl* ctl, const SrvTree* __restrict__ trees,
                  const SrvDesc* descs, SrvCtr* ctrs, SrvDone* done_host, int slots, int stack_cap,
                  unsigned long long wait_ns)

@@ -217,17 +217,69 @@ __device__ __forceinline__ void put_pairs4(int32_t* __restrict__ fid, int32_t* _
 
 // Writes the pairs (bid[first + i], q) to output slots slot0 + i for
 // i < count, skipping slots at or past `cap` (warp-collective).  A contained
-// subtree can hold millions of boxes, so ids move 128 per warp pass as
-// 16-byte vectors: the output is aligned first (up to 3 ids one by one);
-// when the source then sits at another offset within its 16 bytes, each
-// lane's four ids come from its own aligned source vector and its
-// neighbour's (one shuffle per component), so loads and stores both stay
-// 16-byte accesses wherever the reservation starts.  Only aligned vectors
-// inside [bid, bid + first + count) are read.
+// subtree can hold millions of boxes, so the ids are read as 16-byte vectors
+// (128 ids per warp step, kRangeUnroll steps in flight) instead of one 4-byte
+// load per lane; one step keeps the kernels within their register budgets.
+// Where the output is not 16-byte aligned with the source the stores are
+// single; this form needs fewer registers than copy_range_realign (below),
+// and the plain and serving kernels run faster with it.
+constexpr int kRangeUnroll = 1;
+
 __device__ __forceinline__ void copy_range(const int* __restrict__ bid, long long first,
                                            long long count, int32_t* __restrict__ fid,
                                            int32_t* __restrict__ tid, long long slot0,
                                            long long cap, int q)
+{
+  const int lane = (int)lane_id();
+  const int* src = bid + first;
+  // head: ids before the first 16-byte boundary of the source
+  long long head = (long long)((4 - (((uintptr_t)src >> 2) & 3)) & 3);
+  if (head > count) head = count;
+  if (lane < head) put_pair(fid, tid, slot0 + lane, cap, __ldg(src + lane), q);
+  const int4* v = reinterpret_cast<const int4*>(src + head);
+  const long long nv = (count - head) >> 2;
+  const long long s = slot0 + head;
+  for (long long g0 = 0; g0 < nv; g0 += 32 * kRangeUnroll) {
+    int4 r[kRangeUnroll];
+#pragma unroll
+    for (int u = 0; u < kRangeUnroll; u++) {
+      const long long g = g0 + u * 32 + lane;
+      if (g < nv) r[u] = __ldg(v + g);
+    }
+#pragma unroll
+    for (int u = 0; u < kRangeUnroll; u++) {
+      const long long g = g0 + u * 32 + lane;
+      if (g < nv) {
+        const long long sl = s + 4 * g;
+        const uintptr_t al = (uintptr_t)(fid + sl) | (tid ? (uintptr_t)(tid + sl) : (uintptr_t)0);
+        if (sl + 3 < cap && (al & 15) == 0) {
+          __stcs(reinterpret_cast<int4*>(fid + sl), r[u]);
+          if (tid) __stcs(reinterpret_cast<int4*>(tid + sl), make_int4(q, q, q, q));
+        } else {
+          put_pair(fid, tid, sl + 0, cap, r[u].x, q);
+          put_pair(fid, tid, sl + 1, cap, r[u].y, q);
+          put_pair(fid, tid, sl + 2, cap, r[u].z, q);
+          put_pair(fid, tid, sl + 3, cap, r[u].w, q);
+        }
+      }
+    }
+  }
+  // tail: the last (count - head) % 4 ids
+  const long long done = head + 4 * nv;
+  if (lane < count - done) put_pair(fid, tid, slot0 + done + lane, cap, __ldg(src + done + lane), q);
+}
+
+// copy_range with 16-byte stores wherever the reservation starts (the
+// persistent kernel's large-subtree reservations start anywhere in a
+// 16-byte line): the output is aligned first (up to 3 ids one by one); when
+// the source then sits at another offset within its 16 bytes, each lane's
+// four ids come from its own aligned source vector and its neighbour's (one
+// shuffle per component), so loads and stores both stay 16-byte accesses.
+// Only aligned vectors inside [bid, bid + first + count) are read.
+__device__ __forceinline__ void copy_range_realign(const int* __restrict__ bid, long long first,
+                                                   long long count, int32_t* __restrict__ fid,
+                                                   int32_t* __restrict__ tid, long long slot0,
+                                                   long long cap, int q)
 {
   const int lane = (int)lane_id();
   if (count <= 0) return;
