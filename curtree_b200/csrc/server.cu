@@ -411,9 +411,10 @@ struct Server {
   // Copies made while the device loop may run go through pinned host memory
   // (asynchronous on their stream; a pageable copy is staged by the host
   // thread and returns only when it is done).  The loop's stop flag and error
-  // status are mapped words (SrvCtl) that need no copy at all: a copy can
-  // still wait behind other work queued on the device, such as a client's
-  // kernel waiting for SM slots the loop holds.
+  // status are mapped words (SrvCtl) that need no copy at all: any stream
+  // operation can wait behind other work queued on the device (a client's
+  // kernel queued behind the loop, in a hardware queue the streams share),
+  // and the dispatcher must still be able to stop the loop then.
   struct Mailbox {
     SrvState launch;
     unsigned long long published;
@@ -452,10 +453,11 @@ struct Server {
     return (size_t)kSrvWarps * stack_cap * sizeof(FrontierEntry) + (size_t)kSrvWarps * 2 * kStage * 4;
   }
   // All CTA slots but one SM's worth: a loop that held every slot would keep
-  // any other kernel of the process (a client's, a library's) from starting
-  // until it stops, and work queued behind that kernel -- copies included --
-  // would wait too.  The block scheduler spreads the CTAs, so a few SMs keep
-  // a free slot.
+  // any other kernel of the process from starting until it stops.  The block
+  // scheduler spreads the CTAs, so a few SMs keep a free slot, on which a
+  // kernel of another stream runs -- when that stream has a hardware queue of
+  // its own (CUDA_DEVICE_MAX_CONNECTIONS); one that shares the loop's queue
+  // waits for the loop to stop, idle_ms after its last request.
   int grid() const
   {
     int per_sm = 0;

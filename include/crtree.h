@@ -327,9 +327,10 @@ int crt_bbox_free(crt_bbox_f32* d_box);
  * the estimate is re-run with its exact size (overflow-and-retry) before it
  * completes.  Results stay in the arena until crt_server_release.
  * While requests are in flight the device loop holds all but one SM's worth
- * of the GPU's CTA slots: other kernels of the process still run, on the
- * slots left free, and at full speed once the loop has stopped (idle_ms
- * after the last request completes). */
+ * of the GPU's CTA slots.  A kernel of another stream runs beside it on the
+ * slots left free when its stream has a hardware queue of its own
+ * (CUDA_DEVICE_MAX_CONNECTIONS); otherwise it waits until the loop stops,
+ * idle_ms after the last request completes. */
 typedef struct crt_server_s* crt_server;
 
 typedef struct {

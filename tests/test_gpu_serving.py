@@ -122,6 +122,40 @@ def test_tree_with_boxes_not_ordinary(env):
     assert srv.close() == 0
 
 
+def test_client_kernels_while_the_loop_runs(env):
+    """A kernel the client launches while the device loop is up (held up
+    1 s after its last request by idle_ms) may queue behind the loop when its
+    stream shares a hardware queue with the loop's; the loop still stops on
+    time -- the host's stop flag and error word need no CUDA call -- so the
+    kernel runs by then, and the loop ends without a timeout.  Before, the
+    dispatcher's own copies waited behind that kernel, the loop ran on until
+    its bounded wait (device_wait_us, 20 s here) ended it with
+    CRT_ERR_DEVICE_TIMEOUT."""
+    import torch
+    C, Server, trees = env
+    srv, ids = setup_server(C, Server, trees, arena_bytes=1 << 30, idle_ms=1000,
+                            device_wait_us=20_000_000)
+    w = D.mixed_windows(2000, trees[2]["sb"], seed=91, lo=1e-4, hi=3e-2)
+    rid = srv.submit(ids[2], w)
+    cs = []
+    t0 = time.monotonic()
+    while not cs and time.monotonic() - t0 < 30:
+        cs = srv.poll(wait_ms=10)
+    assert cs and cs[0]["status"] == 0
+    got = O.canonical_pairs(*Server.pairs(cs[0]))
+    want = expected(trees, 2, w)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    x = torch.ones(1 << 22, device="cuda")
+    t1 = time.monotonic()
+    for _ in range(20):
+        x = x * 1.0001 + 1.0
+    s = float(x.sum().item())  # waits for this stream only
+    elapsed = time.monotonic() - t1
+    assert s > 0 and elapsed < 3.0, elapsed
+    srv.release(rid)
+    assert srv.close() == 0
+
+
 def test_overflow_and_retry(env):
     C, Server, trees = env
     srv, ids = setup_server(C, Server, trees, pairs_per_window=0.01, output_slack=0.01)
