@@ -78,3 +78,11 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
 def test_opts_defaults():
     o = _lib.default_opts()
     assert o.mode == _lib.CRT_QUERY_PERSISTENT and o.sort_windows == 1 and o.stage_levels == 2 and o.warps_per_window == 1
+
+
+def test_device_bytes_interface():
+    """Device copies in the Python layer go through torch views of raw
+    device ranges (CUDA array interface), not a second CUDA runtime binding."""
+    from curtree_b200.rtree import _DeviceBytes
+    cai = _DeviceBytes(0x1000, 64).__cuda_array_interface__
+    assert cai == {"shape": (64,), "typestr": "|u1", "data": (0x1000, False), "version": 2}
